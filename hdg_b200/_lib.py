@@ -1,0 +1,86 @@
+"""ctypes binding of libhdgx.so (the C ABI declared in include/hdgx.h).
+
+The library is required: importing the compute entry points without it, or calling them
+without a CUDA device, raises.  There is no CPU fallback in this package.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libhdgx.so"
+HDGX_MAX_BND = 16
+
+_dp = ct.c_void_p
+
+
+class HdgxMaster(ct.Structure):
+    _fields_ = [("nd", ct.c_int), ("porder", ct.c_int), ("npv", ct.c_int), ("npf", ct.c_int),
+                ("nfe", ct.c_int), ("ngv", ct.c_int), ("ngf", ct.c_int),
+                ("shapvt", _dp), ("shapvg", _dp), ("shapmv", _dp), ("shapft", _dp),
+                ("shapfg", _dp), ("shapmf", _dp), ("perm", _dp)]
+
+
+class HdgxApp(ct.Structure):
+    _fields_ = [("nd", ct.c_int), ("ncu", ct.c_int), ("nc", ct.c_int), ("localsolve", ct.c_int),
+                ("getdqdg", ct.c_int), ("fc_q", ct.c_double), ("fc_u", ct.c_double), ("tdep", ct.c_int),
+                ("param", ct.c_double * 8), ("nbnd", ct.c_int), ("bcm", ct.c_int * HDGX_MAX_BND),
+                ("bcs", ct.c_double * (HDGX_MAX_BND * 5))]
+
+
+_LIB = None
+
+
+class HdgxError(RuntimeError):
+    pass
+
+
+def lib():
+    """Load libhdgx.so (building it first when the sources are newer)."""
+    global _LIB
+    if _LIB is None:
+        from . import build as _build
+        if _build.needs_build():
+            _build.build()
+        if not LIB_PATH.exists():
+            raise HdgxError(f"{LIB_PATH} is missing; run python -m hdg_b200.build")
+        L = ct.CDLL(str(LIB_PATH))
+        _declare(L)
+        _LIB = L
+    return _LIB
+
+
+def _declare(L):
+    i, d, v, p = ct.c_int, ct.c_double, ct.c_void_p, ct.POINTER
+    L.hdgx_version.restype = i
+    L.hdgx_status_str.restype = ct.c_char_p
+    L.hdgx_status_str.argtypes = [i]
+    L.hdgx_status_count.restype = i
+    L.hdgx_status_count.argtypes = [v, i, v]
+    L.hdgx_elemental.restype = i
+    L.hdgx_elemental.argtypes = [p(HdgxMaster), p(HdgxApp), i] + [v] * 10 + [v]
+    L.hdgx_schur_uq.restype = i
+    L.hdgx_schur_uq.argtypes = [i] * 5 + [v] * 15 + [v]
+    L.hdgx_schur_u.restype = i
+    L.hdgx_schur_u.argtypes = [i] * 5 + [v] * 11 + [v]
+    _declare_optional(L)
+
+
+_OPTIONAL = {}
+
+
+def _declare_optional(L):
+    """Entry points added after the elemental kernel; declared when present."""
+    i, v = ct.c_int, ct.c_void_p
+    for name, res, args in _OPTIONAL.values():
+        if hasattr(L, name):
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+
+
+def check(rc, what):
+    if rc != 0:
+        msg = lib().hdgx_status_str(rc).decode()
+        raise HdgxError(f"{what} failed with status {rc}: {msg}")

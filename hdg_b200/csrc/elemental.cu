@@ -1,0 +1,746 @@
+// elemental.cu -- fused FP64 HDG elemental kernel for sm_100a.
+//
+// One CTA per element (persistent grid-stride over elements), every intermediate in shared
+// memory.  Replaces the reference's chunked pipeline
+//   kernel/hdg_elemental.m:45-203 -> volint.m (volgeom.m) -> faceint.m (facegeom.m)
+//   -> schur_primal.m:52-150 (schur_uq2; C twin kernel/schur_uq.c:42-191)
+// and returns the same four arrays [AE, FE, DUDG, DUDG_DUH] in the same layouts.
+//
+// The algebra is the reference's, reorganised so that the two big coupling operators are
+// never formed:
+//   * B = dRu/dq (BD(:,:,:,ncu+1:end)) only enters through B Mi C, B Mi E and B Mi Rq.  With
+//     B = sum_g sum_i shapvg(r,g,i) shapvt(g,s) wrl_i(g,a,(b,d)) (+ face terms), these become
+//     sum_g sum_i shapvg(r,g,i) sum_d wrl_i(g,a,(b,d)) Z(g,.,d) where Z is Mi C / Mi E / Mi Rq
+//     interpolated to the Gauss points (sum factorisation; cf. the BMiCvol/BMiCface
+//     experiments at kernel/hdg_elemental.m:206-520).
+//   * GK = dRh/d(u,q) is applied to DUDG and DUDG_DUH at the face Gauss points:
+//     (GK X)(a,(n,j)) = sum_g shapfg(n,g) jac_g sum_c FHu(g,a,c) sum_m shapft(g,m) X(perm(m,j),c).
+// H is face-block diagonal and is added directly.  Results equal the reference's up to
+// floating-point summation order.
+#include <cuda_runtime.h>
+#include <math.h>
+#include "hdgx_common.cuh"
+
+namespace hdgx {
+
+struct ElemParams {
+    const double *shapvt, *shapvg, *shapmv, *shapft, *shapfg, *shapmf;
+    const int *perm;
+    PhysConst pc;
+    double fc_q;
+    int nbnd;
+    int bcm[HDGX_MAX_BND];
+    double bcs[HDGX_MAX_BND * 5];
+    int ne;
+    const double *dgnodes, *UDG, *UH, *SH;
+    const int *bf;
+    double *AE, *FE, *DUDG, *DUDG_DUH;
+    int *status;
+};
+
+template <int ND_, int NPV_, int NPF_, int NGV_, int NGF_>
+struct Dims {
+    static constexpr int ND = ND_, NPV = NPV_, NPF = NPF_, NGV = NGV_, NGF = NGF_;
+    static constexpr int NFE = ND + 1, NCU = ND + 2, NC = NCU * (ND + 1);
+    static constexpr int NDF = NPF * NFE, NU = NPV * NCU, NQ = NPV * NC, NH = NCU * NDF;
+    static constexpr int NGT = NGF * NFE;
+};
+
+// Shared-memory plan (in doubles).  "P" = persistent through the element, "X" = the
+// assembly-phase scratch, reused by the DUDG_DUH / AE column tiles at the end.
+template <class D, bool VISC>
+struct Plan {
+    // master tables (loaded once per CTA)
+    static constexpr int t_vt = 0;
+    static constexpr int t_vg = t_vt + D::NGV * D::NPV * (D::ND + 1);
+    static constexpr int t_mv = t_vg + D::NPV * D::NGV * (D::ND + 1);
+    static constexpr int t_ft = t_mv + D::NGV * D::NPV * (D::ND + 1);
+    static constexpr int t_fg = t_ft + D::NGF * D::NPF;
+    static constexpr int t_mf = t_fg + D::NPF * D::NGF;
+    // persistent per element
+    static constexpr int p_dg = t_mf + D::NGF * D::NPF * D::ND;
+    static constexpr int p_udg = p_dg + D::NPV * D::ND;
+    static constexpr int p_uh = p_udg + D::NPV * D::NC;
+    static constexpr int p_SD = p_uh + D::NCU * D::NDF;
+    static constexpr int p_R = p_SD + D::NU * D::NU;              // [NU, 1+NH]
+    static constexpr int p_MiC = p_R + D::NU * (1 + D::NH);       // [NPV, NPV*ND] | MiE | MiRq contiguous
+    static constexpr int p_MiE = p_MiC + D::NPV * D::NPV * D::ND;
+    static constexpr int p_MiRq = p_MiE + D::NPV * D::NDF * D::ND;
+    static constexpr int p_Gp = p_MiRq + D::NPV * D::NCU * D::ND; // [NGT, NCU, NC] jac * dRh-flux/dudg
+    static constexpr int p_Hp = p_Gp + D::NGT * D::NCU * D::NC;   // [NGT, NCU, NCU] jac * dRh-flux/duh
+    static constexpr int p_Rh = p_Hp + D::NGT * D::NCU * D::NCU;
+    static constexpr int p_M = p_Rh + D::NH;
+    static constexpr int p_dudg = p_M + D::NPV * D::NPV;
+    static constexpr int p_end = p_dudg + D::NQ;
+    // assembly scratch
+    static constexpr int x_Xx = p_end;                            // [NGV, ND, ND]
+    static constexpr int x_jac = x_Xx + D::NGV * D::ND * D::ND;
+    static constexpr int x_nl = x_jac + D::NGV;                   // [NGT, ND]
+    static constexpr int x_jf = x_nl + D::NGT * D::ND;
+    static constexpr int x_sh = x_jf + D::NGT;                    // [NPV, NCU*ND] q part of SH
+    static constexpr int x_ug = x_sh + D::NPV * D::NCU * D::ND;   // [NGV, NC]
+    static constexpr int x_fu = x_ug + D::NGV * D::NC;            // [NGT, NC]
+    static constexpr int x_fuh = x_fu + D::NGT * D::NC;           // [NGT, NCU]
+    static constexpr int x_wrk = x_fuh + D::NGT * D::NCU;         // [NGV, ND, NCU]
+    static constexpr int x_wrl = x_wrk + D::NGV * D::ND * D::NCU; // [NGV, ND, NCU, NC]
+    static constexpr int x_FH = x_wrl + D::NGV * D::ND * D::NCU * D::NC;  // [NGT, NCU] jac*fhat
+    static constexpr int x_BH = x_FH + D::NGT * D::NCU;           // [NGT, NCU] jac*(fbou or fhat)
+    static constexpr int x_FHu = x_BH + D::NGT * D::NCU;          // [NGT, NCU, NC] jac*dfhat/dudg
+    static constexpr int x_FHh = x_FHu + D::NGT * D::NCU * D::NC; // [NGT, NCU, NCU] jac*dfhat/duh
+    static constexpr int x_Zc = x_FHh + D::NGT * D::NCU * D::NCU; // [NGV, NPV, ND]
+    static constexpr int x_Ze = x_Zc + (VISC ? D::NGV * D::NPV * D::ND : 0);   // [NGV, NDF, ND]
+    static constexpr int x_Zr = x_Ze + (VISC ? D::NGV * D::NDF * D::ND : 0);   // [NGV, NCU, ND]
+    static constexpr int x_ZFc = x_Zr + (VISC ? D::NGV * D::NCU * D::ND : 0);  // [NGT, NPV, ND]
+    static constexpr int x_ZFe = x_ZFc + (VISC ? D::NGT * D::NPV * D::ND : 0); // [NGT, NDF, ND]
+    static constexpr int x_ZFr = x_ZFe + (VISC ? D::NGT * D::NDF * D::ND : 0); // [NGT, NCU, ND]
+    static constexpr int x_end = x_ZFr + (VISC ? D::NGT * D::NCU * D::ND : 0);
+    static constexpr int x_size = x_end - p_end;
+    // column tiles of DUDG_DUH (reuse the scratch)
+    static constexpr int per_col = D::NQ + D::NGT * D::NC + D::NGT * D::NCU;
+    static constexpr int TILE_RAW = x_size / per_col;
+    static constexpr int TILE = TILE_RAW < 1 ? 1 : (TILE_RAW > D::NH ? D::NH : TILE_RAW);
+    static constexpr int y_X = p_end;
+    static constexpr int y_Xg = y_X + D::NQ * TILE;
+    static constexpr int y_Y = y_Xg + D::NGT * D::NC * TILE;
+    static constexpr int y_end = y_Y + D::NGT * D::NCU * TILE;
+    static constexpr int n_doubles = (x_end > y_end ? x_end : y_end);
+    // integers after the doubles
+    static constexpr int i_perm = 0;                      // [NPF, NFE] 0-based
+    static constexpr int i_invp = D::NPF * D::NFE;        // [NPV, NFE] face-local index or -1
+    static constexpr int i_piv = i_invp + D::NPV * D::NFE;
+    static constexpr int i_pivM = i_piv + D::NU;
+    static constexpr int i_bf = i_pivM + D::NPV;
+    static constexpr int i_bad = i_bf + D::NFE;
+    static constexpr int n_ints = i_bad + 1;
+    static constexpr size_t bytes = sizeof(double) * n_doubles + sizeof(int) * n_ints;
+};
+
+template <class D, bool VISC, int NT>
+__global__ void __launch_bounds__(NT, 1) elemental_kernel(const __grid_constant__ ElemParams P) {
+    using L = Plan<D, VISC>;
+    constexpr int ND = D::ND, NPV = D::NPV, NPF = D::NPF, NGV = D::NGV, NGF = D::NGF;
+    constexpr int NFE = D::NFE, NCU = D::NCU, NC = D::NC, NDF = D::NDF, NU = D::NU;
+    constexpr int NQ = D::NQ, NH = D::NH, NGT = D::NGT;
+    constexpr int NSEED = VISC ? NC : NCU;   // inviscid flux does not depend on q
+    extern __shared__ __align__(16) double sm[];
+    int *si = reinterpret_cast<int *>(sm + L::n_doubles);
+    const int tid = threadIdx.x;
+
+    double *t_vt = sm + L::t_vt, *t_vg = sm + L::t_vg, *t_mv = sm + L::t_mv;
+    double *t_ft = sm + L::t_ft, *t_fg = sm + L::t_fg, *t_mf = sm + L::t_mf;
+    int *perm = si + L::i_perm, *invp = si + L::i_invp;
+
+    // ---- master tables, once per CTA
+    for (int i = tid; i < NGV * NPV * (ND + 1); i += NT) {
+        t_vt[i] = P.shapvt[i];
+        t_vg[i] = P.shapvg[i];
+        t_mv[i] = P.shapmv[i];
+    }
+    for (int i = tid; i < NGF * NPF; i += NT) {
+        t_ft[i] = P.shapft[i];   // value slice of shapft[ngf,npf,nd]
+        t_fg[i] = P.shapfg[i];   // value slice of shapfg[npf,ngf,nd]
+    }
+    for (int i = tid; i < NGF * NPF * ND; i += NT) {
+        const int g = i % NGF, n = (i / NGF) % NPF, k = i / (NGF * NPF);
+        t_mf[i] = P.shapmf[g + NGF * (n + NPF * k)];
+    }
+    for (int i = tid; i < NPF * NFE; i += NT) perm[i] = P.perm[i] - 1;
+    for (int i = tid; i < NPV * NFE; i += NT) invp[i] = -1;
+    __syncthreads();
+    for (int i = tid; i < NPF * NFE; i += NT) invp[perm[i] + NPV * (i / NPF)] = i % NPF;
+    __syncthreads();
+
+    double *s_dg = sm + L::p_dg, *s_udg = sm + L::p_udg, *s_uh = sm + L::p_uh;
+    double *s_SD = sm + L::p_SD, *s_R = sm + L::p_R;
+    double *s_MiC = sm + L::p_MiC, *s_MiE = sm + L::p_MiE, *s_MiRq = sm + L::p_MiRq;
+    double *s_Gp = sm + L::p_Gp, *s_Hp = sm + L::p_Hp, *s_Rh = sm + L::p_Rh, *s_M = sm + L::p_M;
+    double *s_dudg = sm + L::p_dudg;
+    double *x_Xx = sm + L::x_Xx, *x_jac = sm + L::x_jac, *x_nl = sm + L::x_nl, *x_jf = sm + L::x_jf;
+    double *x_sh = sm + L::x_sh, *x_ug = sm + L::x_ug, *x_fu = sm + L::x_fu, *x_fuh = sm + L::x_fuh;
+    double *x_wrk = sm + L::x_wrk, *x_wrl = sm + L::x_wrl, *x_FH = sm + L::x_FH, *x_BH = sm + L::x_BH;
+    double *x_FHu = sm + L::x_FHu, *x_FHh = sm + L::x_FHh;
+    double *x_Zc = sm + L::x_Zc, *x_Ze = sm + L::x_Ze, *x_Zr = sm + L::x_Zr;
+    double *x_ZFc = sm + L::x_ZFc, *x_ZFe = sm + L::x_ZFe, *x_ZFr = sm + L::x_ZFr;
+    int *s_piv = si + L::i_piv, *s_pivM = si + L::i_pivM, *s_bf = si + L::i_bf, *s_bad = si + L::i_bad;
+
+    for (int e = blockIdx.x; e < P.ne; e += gridDim.x) {
+        // ================================================================ load
+        {
+            const double *g_dg = P.dgnodes + (size_t)e * NPV * ND;
+            const double *g_udg = P.UDG + (size_t)e * NPV * NC;
+            const double *g_uh = P.UH + (size_t)e * NCU * NDF;
+            const double *g_sh = P.SH + (size_t)e * NPV * NC;
+            for (int i = tid; i < NPV * ND; i += NT) s_dg[i] = g_dg[i];
+            for (int i = tid; i < NPV * NC; i += NT) s_udg[i] = g_udg[i];
+            for (int i = tid; i < NCU * NDF; i += NT) s_uh[i] = g_uh[i];
+            for (int i = tid; i < NPV * NCU * ND; i += NT) x_sh[i] = g_sh[NPV * NCU + i];
+            if (tid < NFE) s_bf[tid] = P.bf[(size_t)e * NFE + tid];
+            if (tid == 0) *s_bad = 0;
+        }
+        __syncthreads();
+
+        // ====================================================== geometry, traces
+        // volgeom.m:18-61 (Jg(k,m) = dx_m/dxi_k; Xx = adj(Jg)); facegeom.m:20-52.
+        for (int g = tid; g < NGV; g += NT) {
+            double J[ND][ND];
+#pragma unroll
+            for (int k = 0; k < ND; k++)
+#pragma unroll
+                for (int m = 0; m < ND; m++) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int n = 0; n < NPV; n++) t += t_mv[g + NGV * (n + NPV * (k + 1))] * s_dg[n + NPV * m];
+                    J[k][m] = t;
+                }
+            double *X = x_Xx + g;   // X(i,j) at X[NGV*(i + ND*j)]
+            if constexpr (ND == 2) {
+                x_jac[g] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+                X[NGV * (0 + 2 * 0)] = J[1][1];
+                X[NGV * (1 + 2 * 0)] = -J[1][0];
+                X[NGV * (0 + 2 * 1)] = -J[0][1];
+                X[NGV * (1 + 2 * 1)] = J[0][0];
+            } else {
+                x_jac[g] = J[0][0] * J[1][1] * J[2][2] - J[0][0] * J[2][1] * J[1][2] + J[1][0] * J[2][1] * J[0][2]
+                         - J[1][0] * J[0][1] * J[2][2] + J[2][0] * J[0][1] * J[1][2] - J[2][0] * J[1][1] * J[0][2];
+                X[NGV * (0 + 3 * 0)] = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+                X[NGV * (1 + 3 * 0)] = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+                X[NGV * (2 + 3 * 0)] = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+                X[NGV * (0 + 3 * 1)] = J[0][2] * J[2][1] - J[0][1] * J[2][2];
+                X[NGV * (1 + 3 * 1)] = J[0][0] * J[2][2] - J[0][2] * J[2][0];
+                X[NGV * (2 + 3 * 1)] = J[0][1] * J[2][0] - J[0][0] * J[2][1];
+                X[NGV * (0 + 3 * 2)] = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+                X[NGV * (1 + 3 * 2)] = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+                X[NGV * (2 + 3 * 2)] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+            }
+        }
+        for (int gg = tid; gg < NGT; gg += NT) {
+            const int g = gg % NGF, j = gg / NGF;
+            double dp[ND][ND > 1 ? ND - 1 : 1];
+#pragma unroll
+            for (int m = 0; m < ND; m++)
+#pragma unroll
+                for (int k = 0; k < ND - 1; k++) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int n = 0; n < NPF; n++)
+                        t += t_mf[g + NGF * (n + NPF * (k + 1))] * s_dg[perm[n + NPF * j] + NPV * m];
+                    dp[m][k] = t;
+                }
+            if constexpr (ND == 2) {
+                const double jc = sqrt(dp[0][0] * dp[0][0] + dp[1][0] * dp[1][0]);
+                x_jf[gg] = jc;
+                x_nl[gg + NGT * 0] = dp[1][0] / jc;
+                x_nl[gg + NGT * 1] = -dp[0][0] / jc;
+            } else {
+                const double n0 = dp[1][0] * dp[2][1] - dp[2][0] * dp[1][1];
+                const double n1 = dp[2][0] * dp[0][1] - dp[0][0] * dp[2][1];
+                const double n2 = dp[0][0] * dp[1][1] - dp[1][0] * dp[0][1];
+                const double jc = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+                x_jf[gg] = jc;
+                x_nl[gg + NGT * 0] = n0 / jc;
+                x_nl[gg + NGT * 1] = n1 / jc;
+                x_nl[gg + NGT * 2] = n2 / jc;
+            }
+        }
+        // volint.m:31-33 / faceint.m:55-61: solution and trace at the Gauss points
+        for (int i = tid; i < NGV * NC; i += NT) {
+            const int g = i % NGV, c = i / NGV;
+            double t = 0.0;
+#pragma unroll
+            for (int n = 0; n < NPV; n++) t += t_vt[g + NGV * n] * s_udg[n + NPV * c];
+            x_ug[i] = t;
+        }
+        for (int i = tid; i < NGT * NC; i += NT) {
+            const int gg = i % NGT, c = i / NGT, g = gg % NGF, j = gg / NGF;
+            double t = 0.0;
+#pragma unroll
+            for (int n = 0; n < NPF; n++) t += t_ft[g + NGF * n] * s_udg[perm[n + NPF * j] + NPV * c];
+            x_fu[i] = t;
+        }
+        for (int i = tid; i < NGT * NCU; i += NT) {
+            const int gg = i % NGT, a = i / NGT, g = gg % NGF, j = gg / NGF;
+            double t = 0.0;
+#pragma unroll
+            for (int n = 0; n < NPF; n++) t += t_ft[g + NGF * n] * s_uh[a + NCU * (n + NPF * j)];
+            x_fuh[i] = t;
+        }
+        __syncthreads();
+
+        // ============================================= M, C, E (volint.m:43-55, faceint.m:37-48)
+        for (int i = tid; i < NPV * NPV; i += NT) {
+            const int r = i % NPV, s = i / NPV;
+            double t = 0.0;
+#pragma unroll
+            for (int g = 0; g < NGV; g++) t += t_vg[r + NPV * g] * t_vt[g + NGV * s] * x_jac[g];
+            s_M[i] = P.fc_q * t;
+        }
+        for (int i = tid; i < NPV * NPV * ND; i += NT) {
+            const int r = i % NPV, s = (i / NPV) % NPV, d = i / (NPV * NPV);
+            double t = 0.0;
+#pragma unroll
+            for (int g = 0; g < NGV; g++) {
+                double w = 0.0;
+#pragma unroll
+                for (int jd = 0; jd < ND; jd++) w += t_vg[r + NPV * (g + NGV * (jd + 1))] * x_Xx[g + NGV * (d + ND * jd)];
+                t += w * t_vt[g + NGV * s];
+            }
+            s_MiC[i] = t;                          // C(r,s,d), solved in place below
+        }
+        for (int i = tid; i < NPV * NDF * ND; i += NT) {
+            const int r = i % NPV, f = (i / NPV) % NDF, d = i / (NPV * NDF);
+            const int n = f % NPF, j = f / NPF, m = invp[r + NPV * j];
+            double t = 0.0;
+            if (m >= 0) {
+#pragma unroll
+                for (int g = 0; g < NGF; g++) {
+                    const int gg = g + NGF * j;
+                    t += t_fg[m + NPF * g] * t_ft[g + NGF * n] * x_nl[gg + NGT * d] * x_jf[gg];
+                }
+            }
+            s_MiE[i] = t;                          // E(r,(n,j),d)
+        }
+        __syncthreads();
+        // Rq = M (SH/fc_q - q) + C u - E uh   (volint.m:57-60, faceint.m:49-51)
+        for (int i = tid; i < NPV * NCU * ND; i += NT) {
+            const int r = i % NPV, a = (i / NPV) % NCU, d = i / (NPV * NCU);
+            const int cq = NCU + a + NCU * d;
+            double t = 0.0;
+#pragma unroll
+            for (int s = 0; s < NPV; s++)
+                t += s_M[r + NPV * s] * (x_sh[s + NPV * (a + NCU * d)] / P.fc_q - s_udg[s + NPV * cq]);
+#pragma unroll
+            for (int s = 0; s < NPV; s++) t += s_MiC[r + NPV * (s + NPV * d)] * s_udg[s + NPV * a];
+            for (int f = 0; f < NDF; f++) t -= s_MiE[r + NPV * (f + NDF * d)] * s_uh[a + NCU * f];
+            s_MiRq[i] = t;
+        }
+        __syncthreads();
+
+        // ============================ Mi = inv(M): MiC, MiE, MiRq (schur_primal.m:86-91)
+        block_lu<NT>(s_M, NPV, NPV, s_pivM, s_bad);
+        if (tid == 0 && *s_bad) *s_bad = 1;
+        __syncthreads();
+        block_lu_solve<NT>(s_M, NPV, NPV, s_pivM, s_MiC, NPV, NPV * ND + NDF * ND + NCU * ND);
+        __syncthreads();
+
+        // ================================ flux / fhat / fbou at the Gauss points
+        // volume: thread (g, seed); volint.m:81, 241-254
+        for (int i = tid; i < NGV * NSEED; i += NT) {
+            const int g = i % NGV, sd = i / NGV;
+            D1 u[NCU], q[NCU * ND], f[NCU * ND];
+#pragma unroll
+            for (int c = 0; c < NCU; c++) u[c] = {x_ug[g + NGV * c], c == sd ? 1.0 : 0.0};
+#pragma unroll
+            for (int c = 0; c < NCU * ND; c++) q[c] = {x_ug[g + NGV * (NCU + c)], (NCU + c) == sd ? 1.0 : 0.0};
+            ns_flux<ND>(P.pc, u, q, f);
+#pragma unroll
+            for (int id = 0; id < ND; id++)
+#pragma unroll
+                for (int a = 0; a < NCU; a++) {
+                    double w = 0.0, dw = 0.0;
+#pragma unroll
+                    for (int jd = 0; jd < ND; jd++) {
+                        const double xx = x_Xx[g + NGV * (jd + ND * id)];
+                        w += f[a + NCU * jd].v * xx;
+                        dw += f[a + NCU * jd].d * xx;
+                    }
+                    if (sd == 0) x_wrk[g + NGV * (id + ND * a)] = w;
+                    x_wrl[g + NGV * (id + ND * (a + NCU * sd))] = -dw;
+                }
+        }
+        if constexpr (!VISC) {
+            for (int i = tid; i < NGV * ND * NCU * (NC - NCU); i += NT) x_wrl[NGV * ND * NCU * NCU + i] = 0.0;
+        }
+        // faces: thread (gg, seed); fhat.m:49-67 = f(uh,q).n + tau (u - uh)
+        for (int i = tid; i < NGT * NSEED; i += NT) {
+            const int gg = i % NGT, sd = i / NGT;
+            D1 u[NCU], q[NCU * ND], f[NCU * ND];
+#pragma unroll
+            for (int c = 0; c < NCU; c++) u[c] = {x_fuh[gg + NGT * c], c == sd ? 1.0 : 0.0};
+#pragma unroll
+            for (int c = 0; c < NCU * ND; c++) q[c] = {x_fu[gg + NGT * (NCU + c)], (NCU + c) == sd ? 1.0 : 0.0};
+            ns_flux<ND>(P.pc, u, q, f);
+            const double jc = x_jf[gg];
+            const int j = gg / NGF;
+            const int bnd = s_bf[j] < 0;
+            const int ib = bnd ? -s_bf[j] - 1 : 0;
+            const int btype = bnd ? ((ib < P.nbnd) ? P.bcm[ib] : -1) : 0;
+            const bool dir = bnd && btype == 6;
+            if (bnd && btype != 5 && btype != 6) *s_bad = 3;
+#pragma unroll
+            for (int a = 0; a < NCU; a++) {
+                double fn = 0.0, dfn = 0.0;
+#pragma unroll
+                for (int jd = 0; jd < ND; jd++) {
+                    const double nl = x_nl[gg + NGT * jd];
+                    fn += f[a + NCU * jd].v * nl;
+                    dfn += f[a + NCU * jd].d * nl;
+                }
+                if (sd == 0) {
+                    const double fh = fn + P.pc.tau * (x_fu[gg + NGT * a] - x_fuh[gg + NGT * a]);
+                    x_FH[gg + NGT * a] = jc * fh;
+                    const double bh = dir ? (x_fuh[gg + NGT * a] - P.bcs[ib * 5 + a]) : fh;
+                    x_BH[gg + NGT * a] = jc * bh;
+                }
+                if (sd < NCU) {
+                    // dfhat/duh (seed on uh) and dfhat/du = tau I
+                    const double fhh = dfn - (a == sd ? P.pc.tau : 0.0);
+                    const double fhu = (a == sd ? P.pc.tau : 0.0);
+                    x_FHh[gg + NGT * (a + NCU * sd)] = jc * fhh;
+                    x_FHu[gg + NGT * (a + NCU * sd)] = jc * fhu;
+                    s_Hp[gg + NGT * (a + NCU * sd)] = jc * (dir ? (a == sd ? 1.0 : 0.0) : fhh);
+                    s_Gp[gg + NGT * (a + NCU * sd)] = jc * (dir ? 0.0 : fhu);
+                } else {
+                    x_FHu[gg + NGT * (a + NCU * sd)] = jc * dfn;
+                    s_Gp[gg + NGT * (a + NCU * sd)] = jc * (dir ? 0.0 : dfn);
+                }
+            }
+        }
+        if constexpr (!VISC) {
+            for (int i = tid; i < NGT * NCU * (NC - NCU); i += NT) {
+                x_FHu[NGT * NCU * NCU + i] = 0.0;
+                s_Gp[NGT * NCU * NCU + i] = 0.0;
+            }
+        }
+        // Mi C, Mi E, Mi Rq at the volume and face Gauss points (only B couples through them)
+        if constexpr (VISC) {
+            for (int i = tid; i < NGV * NPV * ND; i += NT) {
+                const int g = i % NGV, kd = i / NGV;
+                double t = 0.0;
+#pragma unroll
+                for (int s = 0; s < NPV; s++) t += t_vt[g + NGV * s] * s_MiC[s + NPV * kd];
+                x_Zc[i] = t;
+            }
+            for (int i = tid; i < NGV * NDF * ND; i += NT) {
+                const int g = i % NGV, fd = i / NGV;
+                double t = 0.0;
+#pragma unroll
+                for (int s = 0; s < NPV; s++) t += t_vt[g + NGV * s] * s_MiE[s + NPV * fd];
+                x_Ze[i] = t;
+            }
+            for (int i = tid; i < NGV * NCU * ND; i += NT) {
+                const int g = i % NGV, bd = i / NGV;
+                double t = 0.0;
+#pragma unroll
+                for (int s = 0; s < NPV; s++) t += t_vt[g + NGV * s] * s_MiRq[s + NPV * bd];
+                x_Zr[i] = t;
+            }
+            for (int i = tid; i < NGT * NPV * ND; i += NT) {
+                const int gg = i % NGT, kd = i / NGT, g = gg % NGF, j = gg / NGF;
+                double t = 0.0;
+#pragma unroll
+                for (int n = 0; n < NPF; n++) t += t_ft[g + NGF * n] * s_MiC[perm[n + NPF * j] + NPV * kd];
+                x_ZFc[i] = t;
+            }
+            for (int i = tid; i < NGT * NDF * ND; i += NT) {
+                const int gg = i % NGT, fd = i / NGT, g = gg % NGF, j = gg / NGF;
+                double t = 0.0;
+#pragma unroll
+                for (int n = 0; n < NPF; n++) t += t_ft[g + NGF * n] * s_MiE[perm[n + NPF * j] + NPV * fd];
+                x_ZFe[i] = t;
+            }
+            for (int i = tid; i < NGT * NCU * ND; i += NT) {
+                const int gg = i % NGT, bd = i / NGT, g = gg % NGF, j = gg / NGF;
+                double t = 0.0;
+#pragma unroll
+                for (int n = 0; n < NPF; n++) t += t_ft[g + NGF * n] * s_MiRq[perm[n + NPF * j] + NPV * bd];
+                x_ZFr[i] = t;
+            }
+        }
+        __syncthreads();
+
+        // ========================= SD = D + B Mi C (schur_primal.m:93-110 with volint/faceint)
+        for (int i = tid; i < NU * NU; i += NT) {
+            const int r = i % NPV, a = (i / NPV) % NCU, k = (i / NU) % NPV, b = i / (NU * NPV);
+            double v = 0.0;
+            for (int g = 0; g < NGV; g++) {
+                const double svk = t_vt[g + NGV * k];
+#pragma unroll
+                for (int id = 0; id < ND; id++) {
+                    double w = x_wrl[g + NGV * (id + ND * (a + NCU * b))] * svk;
+                    if constexpr (VISC) {
+#pragma unroll
+                        for (int d = 0; d < ND; d++)
+                            w += x_wrl[g + NGV * (id + ND * (a + NCU * (NCU + b + NCU * d)))] * x_Zc[g + NGV * (k + NPV * d)];
+                    }
+                    v += t_vg[r + NPV * (g + NGV * (id + 1))] * w;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NFE; j++) {
+                const int m = invp[r + NPV * j];
+                if (m < 0) continue;
+                const int nk = invp[k + NPV * j];
+                for (int g = 0; g < NGF; g++) {
+                    const int gg = g + NGF * j;
+                    double w = (nk >= 0) ? t_ft[g + NGF * nk] * x_FHu[gg + NGT * (a + NCU * b)] : 0.0;
+                    if constexpr (VISC) {
+#pragma unroll
+                        for (int d = 0; d < ND; d++)
+                            w += x_FHu[gg + NGT * (a + NCU * (NCU + b + NCU * d))] * x_ZFc[gg + NGT * (k + NPV * d)];
+                    }
+                    v += t_fg[m + NPF * g] * w;
+                }
+            }
+            s_SD[i] = v;
+        }
+        // rhs0 = Ru - B Mi Rq (volint.m:258, faceint.m:306-331; schur_primal.m:95,111)
+        for (int i = tid; i < NU; i += NT) {
+            const int r = i % NPV, a = i / NPV;
+            double v = 0.0;
+            for (int g = 0; g < NGV; g++)
+#pragma unroll
+                for (int id = 0; id < ND; id++) {
+                    double w = x_wrk[g + NGV * (id + ND * a)];
+                    if constexpr (VISC) {
+                        for (int bd = 0; bd < NCU * ND; bd++)
+                            w -= x_wrl[g + NGV * (id + ND * (a + NCU * (NCU + bd)))] * x_Zr[g + NGV * bd];
+                    }
+                    v += t_vg[r + NPV * (g + NGV * (id + 1))] * w;
+                }
+#pragma unroll
+            for (int j = 0; j < NFE; j++) {
+                const int m = invp[r + NPV * j];
+                if (m < 0) continue;
+                for (int g = 0; g < NGF; g++) {
+                    const int gg = g + NGF * j;
+                    double w = -x_FH[gg + NGT * a];
+                    if constexpr (VISC) {
+                        for (int bd = 0; bd < NCU * ND; bd++)
+                            w -= x_FHu[gg + NGT * (a + NCU * (NCU + bd))] * x_ZFr[gg + NGT * bd];
+                    }
+                    v += t_fg[m + NPF * g] * w;
+                }
+            }
+            s_R[i] = v;
+        }
+        // RHS(:, (b,f)) = B Mi E - F   (schur_primal.m:98,118; faceint.m:319-333)
+        for (int i = tid; i < NU * NH; i += NT) {
+            const int r = i % NPV, a = (i / NPV) % NCU, b = (i / NU) % NCU, f = i / (NU * NCU);
+            const int nf = f % NPF, jf = f / NPF;
+            double v = 0.0;
+            if constexpr (VISC) {
+                for (int g = 0; g < NGV; g++)
+#pragma unroll
+                    for (int id = 0; id < ND; id++) {
+                        double w = 0.0;
+#pragma unroll
+                        for (int d = 0; d < ND; d++)
+                            w += x_wrl[g + NGV * (id + ND * (a + NCU * (NCU + b + NCU * d)))] * x_Ze[g + NGV * (f + NDF * d)];
+                        v += t_vg[r + NPV * (g + NGV * (id + 1))] * w;
+                    }
+#pragma unroll
+                for (int j = 0; j < NFE; j++) {
+                    const int m = invp[r + NPV * j];
+                    if (m < 0) continue;
+                    for (int g = 0; g < NGF; g++) {
+                        const int gg = g + NGF * j;
+                        double w = 0.0;
+#pragma unroll
+                        for (int d = 0; d < ND; d++)
+                            w += x_FHu[gg + NGT * (a + NCU * (NCU + b + NCU * d))] * x_ZFe[gg + NGT * (f + NDF * d)];
+                        v += t_fg[m + NPF * g] * w;
+                    }
+                }
+            }
+            const int mf = invp[r + NPV * jf];
+            if (mf >= 0) {
+                double t = 0.0;
+                for (int g = 0; g < NGF; g++)
+                    t += t_fg[mf + NPF * g] * t_ft[g + NGF * nf] * x_FHh[(g + NGF * jf) + NGT * (a + NCU * b)];
+                v -= t;
+            }
+            s_R[NU + i] = v;
+        }
+        // Rh = -(fbou or fhat) integrated on each face (faceint.m:335-339)
+        for (int i = tid; i < NH; i += NT) {
+            const int a = i % NCU, mf = i / NCU, m = mf % NPF, j = mf / NPF;
+            double t = 0.0;
+            for (int g = 0; g < NGF; g++) t += t_fg[m + NPF * g] * x_BH[(g + NGF * j) + NGT * a];
+            s_Rh[i] = -t;
+        }
+        __syncthreads();
+
+        // ================================ LU of SD and the 1 + NH solves (schur_primal.m:111,118)
+        {
+            int bad_before = *s_bad;
+            __syncthreads();
+            block_lu<NT>(s_SD, NU, NU, s_piv, s_bad);
+            if (tid == 0 && *s_bad && !bad_before) *s_bad = 2;
+            __syncthreads();
+            block_lu_solve<NT>(s_SD, NU, NU, s_piv, s_R, NU, 1 + NH);
+            __syncthreads();
+        }
+
+        // ================================ DUDG = [du, MiRq + MiC du] (schur_primal.m:112-116)
+        {
+            double *g_dudg = P.DUDG + (size_t)e * NQ;
+            for (int i = tid; i < NQ; i += NT) {
+                const int r = i % NPV, c = i / NPV;
+                double v;
+                if (c < NCU) {
+                    v = s_R[r + NPV * c];
+                } else {
+                    const int a = (c - NCU) % NCU, d = (c - NCU) / NCU;
+                    v = s_MiRq[r + NPV * (a + NCU * d)];
+#pragma unroll
+                    for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * s_R[s + NPV * a];
+                }
+                s_dudg[i] = v;
+                g_dudg[i] = v;
+            }
+        }
+        __syncthreads();
+        // FE = Rh - GK DUDG (schur_primal.m:143-144), GK applied at the face Gauss points
+        {
+            double *Xg = sm + L::y_Xg;
+            for (int i = tid; i < NGT * NC; i += NT) {
+                const int gg = i % NGT, c = i / NGT, g = gg % NGF, j = gg / NGF;
+                double t = 0.0;
+#pragma unroll
+                for (int m = 0; m < NPF; m++) t += t_ft[g + NGF * m] * s_dudg[perm[m + NPF * j] + NPV * c];
+                Xg[i] = t;
+            }
+            __syncthreads();
+            double *g_fe = P.FE + (size_t)e * NH;
+            for (int i = tid; i < NH; i += NT) {
+                const int a = i % NCU, nf = i / NCU, n = nf % NPF, j = nf / NPF;
+                double t = 0.0;
+                for (int g = 0; g < NGF; g++) {
+                    const int gg = g + NGF * j;
+                    double y = 0.0;
+                    for (int c = 0; c < NC; c++) y += s_Gp[gg + NGT * (a + NCU * c)] * Xg[gg + NGT * c];
+                    t += t_fg[n + NPF * g] * y;
+                }
+                g_fe[i] = s_Rh[i] - t;
+            }
+            __syncthreads();
+        }
+
+        // ============ DUDG_DUH and AE = H + GK DUDG_DUH in column tiles (schur_primal.m:136-147)
+        {
+            constexpr int T = L::TILE;
+            double *yX = sm + L::y_X, *yXg = sm + L::y_Xg, *yY = sm + L::y_Y;
+            double *g_dd = P.DUDG_DUH + (size_t)e * NQ * NH;
+            double *g_ae = P.AE + (size_t)e * NH * NH;
+            for (int k0 = 0; k0 < NH; k0 += T) {
+                const int nt = (NH - k0) < T ? (NH - k0) : T;
+                for (int i = tid; i < NQ * nt; i += NT) {
+                    const int rc = i % NQ, t = i / NQ, k = k0 + t;
+                    const int r = rc % NPV, c = rc / NPV;
+                    const double *dlu = s_R + NU * (1 + k);
+                    double v;
+                    if (c < NCU) {
+                        v = dlu[r + NPV * c];
+                    } else {
+                        const int a = (c - NCU) % NCU, d = (c - NCU) / NCU;
+                        const int b = k % NCU, f = k / NCU;
+                        v = (a == b) ? -s_MiE[r + NPV * (f + NDF * d)] : 0.0;
+#pragma unroll
+                        for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * dlu[s + NPV * a];
+                    }
+                    yX[i] = v;
+                    g_dd[(size_t)NQ * k0 + i] = v;
+                }
+                __syncthreads();
+                for (int i = tid; i < NGT * NC * nt; i += NT) {
+                    const int gg = i % NGT, c = (i / NGT) % NC, t = i / (NGT * NC);
+                    const int g = gg % NGF, j = gg / NGF;
+                    double v = 0.0;
+#pragma unroll
+                    for (int m = 0; m < NPF; m++) v += t_ft[g + NGF * m] * yX[perm[m + NPF * j] + NPV * c + NQ * t];
+                    yXg[i] = v;
+                }
+                __syncthreads();
+                for (int i = tid; i < NGT * NCU * nt; i += NT) {
+                    const int gg = i % NGT, a = (i / NGT) % NCU, t = i / (NGT * NCU);
+                    double v = 0.0;
+                    for (int c = 0; c < NC; c++) v += s_Gp[gg + NGT * (a + NCU * c)] * yXg[gg + NGT * (c + NC * t)];
+                    yY[i] = v;
+                }
+                __syncthreads();
+                for (int i = tid; i < NH * nt; i += NT) {
+                    const int row = i % NH, t = i / NH, k = k0 + t;
+                    const int a = row % NCU, nf = row / NCU, n = nf % NPF, j = nf / NPF;
+                    const int b = k % NCU, fk = k / NCU, nk = fk % NPF, jk = fk / NPF;
+                    double v = 0.0;
+                    for (int g = 0; g < NGF; g++) {
+                        const int gg = g + NGF * j;
+                        double y = yY[gg + NGT * (a + NCU * t)];
+                        if (jk == j) y += t_ft[g + NGF * nk] * s_Hp[gg + NGT * (a + NCU * b)];
+                        v += t_fg[n + NPF * g] * y;
+                    }
+                    g_ae[(size_t)NH * k0 + i] = v;
+                }
+                __syncthreads();
+            }
+        }
+        if (tid == 0 && P.status) P.status[e] = *s_bad;
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ dispatch
+template <class D, bool VISC>
+static int launch_t(const ElemParams &p, cudaStream_t st) {
+    constexpr int NT = 256;
+    using L = Plan<D, VISC>;
+    static_assert(L::TILE >= 1, "tile");
+    const size_t smem = L::bytes;
+    if (smem > 227 * 1024) return -3;
+    auto kern = elemental_kernel<D, VISC, NT>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return -10;
+    int dev = 0, nsm = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
+    if (per_sm < 1) return -11;
+    int grid = nsm * per_sm;
+    if (grid > p.ne) grid = p.ne;
+    if (grid < 1) return 0;
+    kern<<<grid, NT, smem, st>>>(p);
+    err = cudaGetLastError();
+    return err == cudaSuccess ? 0 : -12;
+}
+
+template <class D>
+static int launch_v(const ElemParams &p, bool visc, cudaStream_t st) {
+    return visc ? launch_t<D, true>(p, st) : launch_t<D, false>(p, st);
+}
+
+int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const double *dgnodes,
+                     const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
+                     double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st) {
+    ElemParams p;
+    p.shapvt = m->shapvt; p.shapvg = m->shapvg; p.shapmv = m->shapmv;
+    p.shapft = m->shapft; p.shapfg = m->shapfg; p.shapmf = m->shapmf; p.perm = m->perm;
+    const double gam = app->param[0], re = app->param[2], pr = app->param[3];
+    p.pc.gam1 = gam - 1.0;
+    p.pc.rinv = (re > 0.0 && isfinite(re)) ? 1.0 / re : 0.0;
+    p.pc.kap = p.pc.rinv * gam / (pr * (gam - 1.0));
+    p.pc.tau = app->param[5];
+    p.fc_q = app->fc_q;
+    p.nbnd = app->nbnd;
+    for (int i = 0; i < HDGX_MAX_BND; i++) p.bcm[i] = app->bcm[i];
+    for (int i = 0; i < HDGX_MAX_BND * 5; i++) p.bcs[i] = app->bcs[i];
+    p.ne = ne; p.dgnodes = dgnodes; p.UDG = UDG; p.UH = UH; p.SH = SH; p.bf = bf;
+    p.AE = AE; p.FE = FE; p.DUDG = DUDG; p.DUDG_DUH = DUDG_DUH; p.status = status;
+    const bool visc = p.pc.rinv != 0.0;
+    const int nd = m->nd, po = m->porder;
+    if (nd == 2) {
+        switch (po) {
+            case 1: return launch_v<Dims<2, 3, 2, 3, 2>>(p, visc, st);
+            case 2: return launch_v<Dims<2, 6, 3, 6, 3>>(p, visc, st);
+            case 3: return launch_v<Dims<2, 10, 4, 12, 4>>(p, visc, st);
+            case 4: return launch_v<Dims<2, 15, 5, 16, 5>>(p, visc, st);
+        }
+    } else if (nd == 3) {
+        switch (po) {
+            case 1: return launch_v<Dims<3, 4, 3, 4, 3>>(p, visc, st);
+            case 2: return launch_v<Dims<3, 10, 6, 11, 6>>(p, visc, st);
+        }
+    }
+    return -3;
+}
+
+}  // namespace hdgx

@@ -1,0 +1,182 @@
+// hdgx_common.cuh -- shared device helpers for the HDG elemental kernels (sm_100a, FP64).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/hdgx.h"
+
+namespace hdgx {
+
+// Physics constants derived from hdgx_app.param = [gam, epslm, Re, Pr, Minf, tau].
+struct PhysConst {
+    double gam1, rinv, kap, tau;
+};
+
+// ------------------------------------------------------------------ dual numbers
+// value + one directional derivative; each thread differentiates along one seed.
+struct D1 {
+    double v, d;
+};
+__device__ __forceinline__ D1 dc(double v) { return {v, 0.0}; }
+__device__ __forceinline__ D1 operator+(D1 a, D1 b) { return {a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ D1 operator-(D1 a, D1 b) { return {a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ D1 operator*(D1 a, D1 b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ D1 operator*(D1 a, double s) { return {a.v * s, a.d * s}; }
+__device__ __forceinline__ D1 operator/(D1 a, D1 b) {
+    double ib = 1.0 / b.v;
+    double q = a.v * ib;
+    return {q, (a.d - q * b.d) * ib};
+}
+
+// Compressible Navier-Stokes flux in all ND directions at one point (Euler when rinv = 0).
+// u[NCU] conserved state, q[NCU*ND] gradient slots (component fastest, the reference's
+// sign convention q = -grad u is carried through unchanged).  f[a + NCU*j].
+// Physics: application/FM/ns/flux2d.m / flux3d.m (flux_ns2d.c / flux_ns3d.c).
+template <int ND>
+__device__ __forceinline__ void ns_flux(const PhysConst &pc, const D1 *u, const D1 *q, D1 *f) {
+    constexpr int NCU = ND + 2;
+    const D1 r = u[0], rE = u[NCU - 1];
+    D1 vel[ND];
+    D1 ke = dc(0.0);
+#pragma unroll
+    for (int i = 0; i < ND; i++) {
+        vel[i] = u[1 + i] / r;
+        ke = ke + vel[i] * u[1 + i];
+    }
+    const D1 p = (rE - ke * 0.5) * pc.gam1;
+    const D1 h = (rE + p) / r;
+    if (pc.rinv == 0.0) {
+#pragma unroll
+        for (int j = 0; j < ND; j++) {
+            f[0 + NCU * j] = u[1 + j];
+#pragma unroll
+            for (int i = 0; i < ND; i++) {
+                D1 t = u[1 + i] * vel[j];
+                if (i == j) t = t + p;
+                f[(1 + i) + NCU * j] = t;
+            }
+            f[(NCU - 1) + NCU * j] = h * u[1 + j];
+        }
+        return;
+    }
+    const D1 ri = dc(1.0) / r;
+    D1 gv[ND][ND];
+#pragma unroll
+    for (int i = 0; i < ND; i++)
+#pragma unroll
+        for (int j = 0; j < ND; j++) gv[i][j] = (q[(1 + i) + NCU * j] - vel[i] * q[NCU * j]) * ri;
+    D1 div = dc(0.0);
+#pragma unroll
+    for (int i = 0; i < ND; i++) div = div + gv[i][i];
+    D1 v2 = dc(0.0);
+#pragma unroll
+    for (int i = 0; i < ND; i++) v2 = v2 + vel[i] * vel[i];
+#pragma unroll
+    for (int j = 0; j < ND; j++) {
+        D1 tauj[ND];
+#pragma unroll
+        for (int i = 0; i < ND; i++) {
+            D1 t = gv[i][j] + gv[j][i];
+            if (i == j) t = t - div * (2.0 / 3.0);
+            tauj[i] = t * pc.rinv;
+        }
+        D1 vdv = dc(0.0);
+#pragma unroll
+        for (int i = 0; i < ND; i++) vdv = vdv + vel[i] * gv[i][j];
+        const D1 qr = q[NCU * j];
+        const D1 pj = (q[(NCU - 1) + NCU * j] - v2 * 0.5 * qr - r * vdv) * pc.gam1;
+        const D1 Tj = (pj * r - p * qr) / (r * r);
+        f[0 + NCU * j] = u[1 + j];
+        D1 e = h * u[1 + j];
+#pragma unroll
+        for (int i = 0; i < ND; i++) {
+            D1 t = u[1 + i] * vel[j] + tauj[i];
+            if (i == j) t = t + p;
+            f[(1 + i) + NCU * j] = t;
+            e = e + vel[i] * tauj[i];
+        }
+        f[(NCU - 1) + NCU * j] = e + Tj * pc.kap;
+    }
+}
+
+// --------------------------------------------------------------- block helpers
+template <int NT>
+__device__ __forceinline__ double block_reduce_max_abs(double v, double *red) {
+    // not used on hot paths; kept simple
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double m = 0.0;
+    for (int w = 0; w < NT / 32; w++) m = fmax(m, red[w]);
+    __syncthreads();
+    return m;
+}
+
+// In-place LU with partial pivoting of column-major A[n x n] (leading dimension lda) in
+// shared memory by the whole block.  piv[k] = pivot row chosen at step k.  Returns
+// nonzero (k+1) in *bad when a pivot is zero or not finite.  Warp 0 picks the pivot.
+template <int NT>
+__device__ void block_lu(double *A, int n, int lda, int *piv, int *bad) {
+    for (int k = 0; k < n; k++) {
+        if (threadIdx.x < 32) {
+            double best = -1.0;
+            int bi = k;
+            for (int i = k + threadIdx.x; i < n; i += 32) {
+                double v = fabs(A[i + lda * k]);
+                if (v > best) { best = v; bi = i; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            if (threadIdx.x == 0) {
+                piv[k] = bi;
+                if (!(best > 0.0) || !isfinite(best)) { if (*bad == 0) *bad = k + 1; }
+            }
+        }
+        __syncthreads();
+        const int p = piv[k];
+        if (p != k) {
+            for (int j = threadIdx.x; j < n; j += NT) {
+                double t = A[k + lda * j];
+                A[k + lda * j] = A[p + lda * j];
+                A[p + lda * j] = t;
+            }
+            __syncthreads();
+        }
+        const double akk = A[k + lda * k];
+        const double inv = (akk != 0.0) ? 1.0 / akk : 0.0;
+        for (int i = k + 1 + threadIdx.x; i < n; i += NT) A[i + lda * k] *= inv;
+        __syncthreads();
+        const int m = n - k - 1;
+        for (int t = threadIdx.x; t < m * m; t += NT) {
+            const int i = k + 1 + t % m, j = k + 1 + t / m;
+            A[i + lda * j] -= A[i + lda * k] * A[k + lda * j];
+        }
+        __syncthreads();
+    }
+}
+
+// Solve A X = B for ncols right-hand sides (columns of B, leading dimension ldb) with the
+// factors of block_lu; one thread per column.
+template <int NT>
+__device__ void block_lu_solve(const double *LU, int n, int lda, const int *piv, double *B, int ldb, int ncols) {
+    for (int c = threadIdx.x; c < ncols; c += NT) {
+        double *b = B + (size_t)ldb * c;
+        for (int k = 0; k < n; k++) {
+            const int p = piv[k];
+            if (p != k) { double t = b[k]; b[k] = b[p]; b[p] = t; }
+        }
+        for (int k = 0; k < n; k++) {
+            const double bk = b[k];
+            for (int i = k + 1; i < n; i++) b[i] -= LU[i + lda * k] * bk;
+        }
+        for (int k = n - 1; k >= 0; k--) {
+            const double bk = b[k] / LU[k + lda * k];
+            b[k] = bk;
+            for (int i = 0; i < k; i++) b[i] -= LU[i + lda * k] * bk;
+        }
+    }
+}
+
+}  // namespace hdgx

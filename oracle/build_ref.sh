@@ -1,0 +1,36 @@
+#!/usr/bin/env bash
+# Compile the reference's own C sources for this path, where they lie in the reference
+# tree, into oracle/_ref/ (git-ignored; travels with the snapshot).  Test infrastructure:
+#   schur_uq.so / schur_u.so / arraymul.so : kernel/schur_uq.c, kernel/schur_u.c,
+#       kernel/arraymul.c + the MEX emulation in oracle/refshim, against numpy's ILP64
+#       OpenBLAS (MATLAB's BLAS ABI uses ptrdiff_t integers);
+#   libref_ns.so : application/FM/ns/{flux,fhat}_ns{2,3}d.c and
+#       application/FM/euler/{flux,fhat}_euler{2,3}d.c (generated point kernels).
+# Usage: oracle/build_ref.sh [reference-root]
+set -euo pipefail
+REF=${1:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+[ -d "$REF/kernel" ] || { echo "reference tree not found at $REF; skipping"; exit 0; }
+mkdir -p "$OUT"
+OB=$(python -c 'import numpy, glob, os; print(glob.glob(os.path.join(os.path.dirname(numpy.__file__), os.pardir, "numpy.libs", "libscipy_openblas64_*.so"))[0])')
+OBDIR=$(dirname "$OB"); OBNAME=$(basename "$OB")
+for f in schur_uq schur_u arraymul; do
+  gcc -O2 -fPIC -shared -w -I"$HERE/refshim" -o "$OUT/$f.so" "$REF/kernel/$f.c" "$HERE/refshim/mexharness.c" \
+      "$OB" -Wl,-rpath,"$OBDIR" -lm
+done
+TMP=$(mktemp -d)
+cat > "$TMP/ns.c" <<CEOF
+#include <math.h>
+#include "$REF/application/FM/ns/flux_ns2d.c"
+#include "$REF/application/FM/ns/flux_ns3d.c"
+#include "$REF/application/FM/ns/fhat_ns2d.c"
+#include "$REF/application/FM/ns/fhat_ns3d.c"
+#include "$REF/application/FM/euler/flux_euler2d.c"
+#include "$REF/application/FM/euler/flux_euler3d.c"
+#include "$REF/application/FM/euler/fhat_euler2d.c"
+#include "$REF/application/FM/euler/fhat_euler3d.c"
+CEOF
+gcc -O2 -fPIC -shared -w -std=gnu99 -o "$OUT/libref_ns.so" "$TMP/ns.c" -lm
+rm -rf "$TMP"
+echo "built: $(ls "$OUT")"

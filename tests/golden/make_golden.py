@@ -1,0 +1,93 @@
+"""Generate the committed golden fixtures from the reference (run in a tree that has it).
+
+* master_tri_p2.npz  -- master/testpython.mat (p=2, pgauss=4, triangle), fields as stored.
+* ref_physics.npz    -- outputs of the reference's generated point kernels
+                        application/FM/ns/{flux,fhat}_ns{2,3}d.c and application/FM/euler/
+                        {flux,fhat}_euler{2,3}d.c (compiled into oracle/_ref)
+                        on seeded random states.
+* ref_schur.npz      -- outputs of the reference MEX sources kernel/schur_uq.c and
+                        kernel/schur_u.c (compiled into oracle/_ref with the MEX emulation)
+                        on the elemental blocks of a 2D Euler p=2 case (8 elements) and a
+                        2D Navier-Stokes p=3 case (8 elements).
+
+Usage: python tests/golden/make_golden.py [reference-root]
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+import scipy.io as sio
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+OUT = Path(__file__).resolve().parent
+
+MASTER_FIELDS = ["nd", "porder", "plocvl", "plocfc", "perm", "gpvl", "gwvl", "shapvl", "gpfc", "gwfc",
+                 "shapfc", "shapvgdotshapvl", "shapvt", "shapvg", "shapfgdotshapfc", "shapft", "shapfg"]
+
+
+def _master(struct):
+    out = {}
+    for k in MASTER_FIELDS:
+        if k in struct.dtype.names:
+            out[k] = np.array(struct[k], dtype=np.float64)
+    return out
+
+
+def main(ref):
+    ref = Path(ref)
+    from oracle import oracle as O
+    from hdg_b200 import configs
+
+    d = sio.loadmat(ref / "master/testpython.mat")
+    np.savez_compressed(OUT / "master_tri_p2.npz", **_master(d["masterm"][0, 0]))
+
+    rng = np.random.default_rng(20261203)
+    phys = {}
+    for nd in (2, 3):
+        ncu = nd + 2; nc = ncu * (nd + 1); ng = 40
+        udg = 0.05 * rng.standard_normal((ng, nc))
+        udg[:, 0] = 1.0 + 0.1 * rng.random(ng)
+        udg[:, 1:nd + 1] = rng.standard_normal((ng, nd))
+        udg[:, ncu - 1] = 5.0 + rng.random(ng)
+        nl = rng.standard_normal((ng, nd)); nl /= np.linalg.norm(nl, axis=1, keepdims=True)
+        uh = udg[:, :ncu] + 0.01 * rng.standard_normal((ng, ncu))
+        for tag, param in (("ns", [1.4, 0.0, 1000.0, 0.72, 0.3, 2.0]), ("euler", [1.4, 0.0, np.inf, 0.72, 0.5, 2.0])):
+            param = np.array(param)
+            # Euler: application/FM/euler kernels on the u-only state (nc = ncu)
+            src = udg if tag == "ns" else np.asfortranarray(udg[:, :ncu])
+            f, fu = O.ref_flux(nd, param, src, tag)
+            fh, fhu, fhh = O.ref_fhat(nd, param, nl, src, uh, tag)
+            p = f"{tag}{nd}d_"
+            phys.update({p + "param": param, p + "udg": udg, p + "nl": nl, p + "uh": uh, p + "f": f,
+                         p + "f_udg": fu, p + "fh": fh, p + "fh_udg": fhu, p + "fh_uh": fhh})
+    np.savez_compressed(OUT / "ref_physics.npz", **phys)
+
+    sch = {}
+    for tag, P in (("euler2d", configs.c1(n=2, porder=2)), ("ns2d", configs.c2(n=1, porder=3))):
+        m, a = P.master, P.app
+        blk = O.hdg_elemental(m, a, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), P.SH, intermediates=True)
+        ne = P.mesh.ne; npv = m.npv; nc = a.nc; ncu = a.ncu; ndf = m.npf * m.nfe
+        keys = ("M", "C", "E", "BD", "F", "GK", "H", "Rq", "Ru", "Rh")
+        outs = O.ref_mex("schur_uq.so", [blk[k].copy() for k in keys],
+                         [(npv, nc, ne), (npv, nc, ncu, ndf, ne), (ncu, ndf, ncu, ndf, ne), (ncu, ndf, ne)])
+        for k in keys:
+            sch[f"{tag}_{k}"] = blk[k]
+        for k, v in zip(("DUDG", "DUDG_DUH", "AE", "FE"), outs):
+            sch[f"{tag}_uq_{k}"] = v
+        # u-only form: D block and the u columns of GK
+        BDu = np.asfortranarray(blk["BD"][:, :, :, :ncu, :])
+        GKu = np.asfortranarray(blk["GK"][:, :, :, :ncu, :])
+        outs = O.ref_mex("schur_u.so", [BDu, blk["F"].copy(), GKu, blk["H"].copy(), blk["Ru"].copy(), blk["Rh"].copy()],
+                         [(npv, ncu, ne), (npv, ncu, ncu, ndf, ne), (ncu, ndf, ncu, ndf, ne), (ncu, ndf, ne)])
+        sch[f"{tag}_BDu"] = BDu
+        sch[f"{tag}_GKu"] = GKu
+        for k, v in zip(("DUDG", "DUDG_DUH", "AE", "FE"), outs):
+            sch[f"{tag}_u_{k}"] = v
+    np.savez_compressed(OUT / "ref_schur.npz", **sch)
+    for f in sorted(OUT.glob("*.npz")):
+        print(f.name, f.stat().st_size)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,67 @@
+"""Host set-up checks: mesh sizes of the workloads, connectivity and geometry invariants."""
+import numpy as np
+import pytest
+
+from hdg_b200 import configs
+from hdg_b200.master import mkmaster
+from hdg_b200.mesh import mkmesh_cube, mkmesh_square
+
+
+def test_square_mesh_counts_c1():
+    m = mkmesh_square(17, 17, 2, 0, 10.0, 10.0)
+    assert m.ne == 512 and m.nf == 800 and m.cbsr_nblks == 3872
+    assert m.elcon.shape == (9, 512) and m.nsiz == 2400
+
+
+def test_block_crs_has_diagonal_first():
+    m = mkmesh_square(5, 5, 2)
+    for i in range(m.nf):
+        assert m.cbsr_colind[m.cbsr_rowpts[i]] == i + 1
+
+
+@pytest.mark.parametrize("mk", [lambda: mkmesh_square(6, 5, 3), lambda: mkmesh_cube(3, 3, 3, 2)])
+def test_elcon_shared_nodes_coincide(mk):
+    m = mk()
+    nd = m.nd
+    ms = mkmaster(nd, m.porder)
+    npf, nfe = ms.perm.shape
+    pos = {}
+    for e in range(m.ne):
+        for j in range(nfe):
+            for a in range(npf):
+                x = m.dgnodes[ms.perm[a, j] - 1, :, e]
+                k = m.elcon[a + npf * j, e]
+                if k in pos:
+                    assert np.allclose(pos[k], x, atol=1e-12)
+                else:
+                    pos[k] = x
+    assert len(pos) == m.nsiz
+
+
+@pytest.mark.parametrize("nd,po", [(2, 1), (2, 3), (3, 1), (3, 2)])
+def test_face_normals_point_outward(nd, po):
+    """Normals from facegeom's formula (facegeom.m:40-49) point away from the element."""
+    m = mkmesh_square(3, 3, po) if nd == 2 else mkmesh_cube(2, 2, 2, po)
+    ms = mkmaster(nd, po)
+    for e in range(m.ne):
+        dg = m.dgnodes[:, :, e]
+        cen = dg.mean(axis=0)
+        for j in range(ms.nfe):
+            pn = dg[ms.perm[:, j] - 1]
+            g = 0
+            dp = np.stack([ms.shapmf[g, :, k + 1] @ pn for k in range(nd - 1)], axis=1)  # [nd, nd-1]
+            if nd == 2:
+                nl = np.array([dp[1, 0], -dp[0, 0]])
+            else:
+                nl = np.cross(dp[:, 0], dp[:, 1])
+            fc = ms.shapmf[g, :, 0] @ pn
+            assert nl @ (fc - cen) > 0
+
+
+def test_partition_of_unity_and_quadrature():
+    for nd, po in [(2, 1), (2, 2), (2, 3), (2, 4), (3, 1), (3, 2), (3, 3)]:
+        ms = mkmaster(nd, po)
+        assert np.allclose(ms.shapvl[:, :, 0].sum(axis=0), 1.0, atol=1e-12)
+        assert np.allclose(ms.shapvl[:, :, 1:].sum(axis=0), 0.0, atol=1e-10)
+        vol = 0.5 if nd == 2 else 1.0 / 6.0
+        assert abs(ms.gwvl.sum() - vol) < 1e-12

@@ -145,7 +145,7 @@ def _ref(name):
 def ref_mex(soname, inputs, out_shapes):
     """Run a reference mexFunction (oracle/_ref/<soname>) on Fortran-ordered inputs."""
     L = _ref(soname)
-    ins = [_f(x) for x in inputs]
+    ins = [np.array(x, dtype=np.float64, order="F", copy=True) for x in inputs]   # MEX overwrites inputs
     ptrs = (_dp * len(ins))(*[_p(x) for x in ins])
     ndims = (ct.c_int * len(ins))(*[x.ndim for x in ins])
     dims = [d for x in ins for d in x.shape]

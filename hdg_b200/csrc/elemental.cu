@@ -103,20 +103,25 @@ struct Plan {
     static constexpr int y_Xg = y_X + D::NQ * TILE;
     static constexpr int y_Y = y_Xg + D::NGT * D::NC * TILE;
     static constexpr int y_end = y_Y + D::NGT * D::NCU * TILE;
-    static constexpr int n_doubles = (x_end > y_end ? x_end : y_end);
+    static constexpr int d_slots = (x_end > y_end ? x_end : y_end);   // 3 x u64 pivot slots
+    static constexpr int n_doubles = d_slots + 4;
     // integers after the doubles
     static constexpr int i_perm = 0;                      // [NPF, NFE] 0-based
     static constexpr int i_invp = D::NPF * D::NFE;        // [NPV, NFE] face-local index or -1
     static constexpr int i_piv = i_invp + D::NPV * D::NFE;
     static constexpr int i_pivM = i_piv + D::NU;
-    static constexpr int i_bf = i_pivM + D::NPV;
+    static constexpr int i_rowused = i_pivM + D::NPV;
+    static constexpr int i_bf = i_rowused + D::NU;
     static constexpr int i_bad = i_bf + D::NFE;
     static constexpr int n_ints = i_bad + 1;
     static constexpr size_t bytes = sizeof(double) * n_doubles + sizeof(int) * n_ints;
 };
 
+template <class D, bool VISC>
+constexpr int min_blocks() { return Plan<D, VISC>::bytes <= 110 * 1024 ? 2 : 1; }
+
 template <class D, bool VISC, int NT>
-__global__ void __launch_bounds__(NT, 1) elemental_kernel(const __grid_constant__ ElemParams P) {
+__global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(const __grid_constant__ ElemParams P) {
     using L = Plan<D, VISC>;
     constexpr int ND = D::ND, NPV = D::NPV, NPF = D::NPF, NGV = D::NGV, NGF = D::NGF;
     constexpr int NFE = D::NFE, NCU = D::NCU, NC = D::NC, NDF = D::NDF, NU = D::NU;
@@ -162,6 +167,8 @@ __global__ void __launch_bounds__(NT, 1) elemental_kernel(const __grid_constant_
     double *x_Zc = sm + L::x_Zc, *x_Ze = sm + L::x_Ze, *x_Zr = sm + L::x_Zr;
     double *x_ZFc = sm + L::x_ZFc, *x_ZFe = sm + L::x_ZFe, *x_ZFr = sm + L::x_ZFr;
     int *s_piv = si + L::i_piv, *s_pivM = si + L::i_pivM, *s_bf = si + L::i_bf, *s_bad = si + L::i_bad;
+    int *s_rowused = si + L::i_rowused;
+    unsigned long long *s_slot = reinterpret_cast<unsigned long long *>(sm + L::d_slots);
 
     for (int e = blockIdx.x; e < P.ne; e += gridDim.x) {
         // ================================================================ load
@@ -316,10 +323,10 @@ __global__ void __launch_bounds__(NT, 1) elemental_kernel(const __grid_constant_
         __syncthreads();
 
         // ============================ Mi = inv(M): MiC, MiE, MiRq (schur_primal.m:86-91)
-        block_lu<NT>(s_M, NPV, NPV, s_pivM, s_bad);
+        // M is SPD (exact quadrature of phi phi jac): eliminate without pivoting
+        block_gauss_jordan<NT, false>(s_M, NPV, s_MiC, NPV, NPV, NPV * ND + NDF * ND + NCU * ND,
+                                      s_pivM, s_rowused, s_slot, s_bad);
         if (tid == 0 && *s_bad) *s_bad = 1;
-        __syncthreads();
-        block_lu_solve<NT>(s_M, NPV, NPV, s_pivM, s_MiC, NPV, NPV * ND + NDF * ND + NCU * ND);
         __syncthreads();
 
         // ================================ flux / fhat / fbou at the Gauss points
@@ -564,10 +571,8 @@ __global__ void __launch_bounds__(NT, 1) elemental_kernel(const __grid_constant_
         {
             int bad_before = *s_bad;
             __syncthreads();
-            block_lu<NT>(s_SD, NU, NU, s_piv, s_bad);
+            block_gauss_jordan<NT, true>(s_SD, NU, s_R, NU, NU, 1 + NH, s_piv, s_rowused, s_slot, s_bad);
             if (tid == 0 && *s_bad && !bad_before) *s_bad = 2;
-            __syncthreads();
-            block_lu_solve<NT>(s_SD, NU, NU, s_piv, s_R, NU, 1 + NH);
             __syncthreads();
         }
 
@@ -578,12 +583,12 @@ __global__ void __launch_bounds__(NT, 1) elemental_kernel(const __grid_constant_
                 const int r = i % NPV, c = i / NPV;
                 double v;
                 if (c < NCU) {
-                    v = s_R[r + NPV * c];
+                    v = s_R[s_piv[r + NPV * c]];
                 } else {
                     const int a = (c - NCU) % NCU, d = (c - NCU) / NCU;
                     v = s_MiRq[r + NPV * (a + NCU * d)];
 #pragma unroll
-                    for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * s_R[s + NPV * a];
+                    for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * s_R[s_piv[s + NPV * a]];
                 }
                 s_dudg[i] = v;
                 g_dudg[i] = v;
@@ -630,13 +635,13 @@ __global__ void __launch_bounds__(NT, 1) elemental_kernel(const __grid_constant_
                     const double *dlu = s_R + NU * (1 + k);
                     double v;
                     if (c < NCU) {
-                        v = dlu[r + NPV * c];
+                        v = dlu[s_piv[r + NPV * c]];
                     } else {
                         const int a = (c - NCU) % NCU, d = (c - NCU) / NCU;
                         const int b = k % NCU, f = k / NCU;
                         v = (a == b) ? -s_MiE[r + NPV * (f + NDF * d)] : 0.0;
 #pragma unroll
-                        for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * dlu[s + NPV * a];
+                        for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * dlu[s_piv[s + NPV * a]];
                     }
                     yX[i] = v;
                     g_dd[(size_t)NQ * k0 + i] = v;

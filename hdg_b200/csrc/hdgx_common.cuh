@@ -179,4 +179,72 @@ __device__ void block_lu_solve(const double *LU, int n, int lda, const int *piv,
     }
 }
 
+
+// Gauss-Jordan elimination with partial pivoting on the augmented system [A | B] held in
+// shared memory (A: n x n, lda; B: n x nrhs, ldb), one __syncthreads per step.  The pivot
+// search for step k+1 is fused into the step-k update: the threads that update column k+1
+// of not-yet-pivoted rows post (|value| bits, row) into a 64-bit atomicMax slot (three
+// rotating slots make one barrier per step sufficient).  Rows are never swapped; pivrow[k]
+// records the physical row that carries unknown k.  On return B's row pivrow[k] holds the
+// solution component k (already divided by the pivot).  *bad is set to k+1 when the pivot
+// of step k is zero or not finite (the elimination still runs to completion).
+// PIVOT = false eliminates in natural order (pivrow[k] = k), for SPD matrices such as M.
+// Work per step: (n-1) rows x (n-k-1+nrhs) columns.
+template <int NT, bool PIVOT = true>
+__device__ void block_gauss_jordan(double *A, int lda, double *B, int ldb, int n, int nrhs,
+                                   int *pivrow, int *rowused, unsigned long long *slot, int *bad) {
+    const int tid = threadIdx.x;
+    constexpr unsigned long long RMASK = 0x3FFull;   // rows < 1024
+    for (int r = tid; r < n; r += NT) rowused[r] = 0;
+    if (tid < 3) slot[tid] = 0ull;
+    __syncthreads();
+    // pivot for step 0
+    for (int r = tid; r < n && PIVOT; r += NT) {
+        const double v = fabs(A[r]);
+        unsigned long long key = ((unsigned long long)__double_as_longlong(v) & ~RMASK) | (unsigned long long)r;
+        atomicMax(&slot[0], key);
+    }
+    __syncthreads();
+    for (int k = 0; k < n; k++) {
+        const unsigned long long key = slot[k % 3];
+        const int p = PIVOT ? (int)(key & RMASK) : k;
+        const double piv = A[p + lda * k];
+        if (tid == 0) {
+            pivrow[k] = p;
+            rowused[p] = 1;
+            slot[(k + 2) % 3] = 0ull;
+            if (!(fabs(piv) > 0.0) || !isfinite(piv)) { if (*bad == 0) *bad = k + 1; }
+        }
+        const double ipiv = (piv != 0.0) ? 1.0 / piv : 0.0;
+        const int na = n - k - 1;             // remaining A columns k+1..n-1
+        const int nc = na + nrhs;
+        unsigned long long* nxt = &slot[(k + 1) % 3];
+        for (int t = tid; t < n * nc; t += NT) {
+            const int r = t % n, jj = t / n;
+            if (r == p) continue;
+            const double l = A[r + lda * k] * ipiv;
+            if (jj < na) {
+                const int j = k + 1 + jj;
+                const double v = A[r + lda * j] - l * A[p + lda * j];
+                A[r + lda * j] = v;
+                if (PIVOT && jj == 0 && !rowused[r]) {
+                    unsigned long long kk = ((unsigned long long)__double_as_longlong(fabs(v)) & ~RMASK) | (unsigned long long)r;
+                    atomicMax(nxt, kk);
+                }
+            } else {
+                const int j = jj - na;
+                B[r + ldb * j] -= l * B[p + ldb * j];
+            }
+        }
+        __syncthreads();
+    }
+    // scale: unknown k lives in row pivrow[k]
+    for (int t = tid; t < n * nrhs; t += NT) {
+        const int k = t % n, j = t / n;
+        const int r = pivrow[k];
+        B[r + ldb * j] /= A[r + lda * k];
+    }
+    __syncthreads();
+}
+
 }  // namespace hdgx

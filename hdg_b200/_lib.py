@@ -29,6 +29,15 @@ class HdgxApp(ct.Structure):
                 ("bcs", ct.c_double * (HDGX_MAX_BND * 5))]
 
 
+class HdgxBsr(ct.Structure):
+    _fields_ = [("nf", ct.c_int), ("bs", ct.c_int), ("nnzb", ct.c_longlong), ("rowpts", _dp), ("colind", _dp),
+                ("ncolors", ct.c_int), ("color_ptr", _dp), ("color_rows", _dp), ("pos", _dp)]
+
+
+class HdgxAssemblyMap(ct.Structure):
+    _fields_ = [("blk_e", _dp), ("blk_ab", _dp), ("blk_row", _dp), ("face_e", _dp), ("face_a", _dp)]
+
+
 _LIB = None
 
 
@@ -64,6 +73,23 @@ def _declare(L):
     L.hdgx_schur_uq.argtypes = [i] * 5 + [v] * 15 + [v]
     L.hdgx_schur_u.restype = i
     L.hdgx_schur_u.argtypes = [i] * 5 + [v] * 11 + [v]
+    B, M = p(HdgxBsr), p(HdgxAssemblyMap)
+    L.hdgx_gather_uh.restype = i
+    L.hdgx_gather_uh.argtypes = [i, i, i, v, v, v, v]
+    L.hdgx_globalassembly.restype = i
+    L.hdgx_globalassembly.argtypes = [B, M, i, i, i, v, v, v, v, v, v]
+    L.hdgx_matvec.restype = i
+    L.hdgx_matvec.argtypes = [B, v, v, v, v]
+    L.hdgx_bilu0_factor.restype = i
+    L.hdgx_bilu0_factor.argtypes = [B, v, v, v]
+    L.hdgx_bilu0_apply.restype = i
+    L.hdgx_bilu0_apply.argtypes = [B, v, v, v, v, v]
+    L.hdgx_gmres_workspace_bytes.restype = ct.c_size_t
+    L.hdgx_gmres_workspace_bytes.argtypes = [B, i]
+    L.hdgx_gmres_bilu0.restype = i
+    L.hdgx_gmres_bilu0.argtypes = [B, v, v, v, v, i, d, i, p(i), p(i), p(d), v, v, v]
+    L.hdgx_backsub.restype = i
+    L.hdgx_backsub.argtypes = [i, i, i, i, i, v, v, v, v, v, v]
     _declare_optional(L)
 
 

@@ -1,0 +1,240 @@
+// capi_trace.cu -- extern "C" entry points of the condensed-system path (include/hdgx.h).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <vector>
+#include "hdgx_common.cuh"
+
+namespace hdgx {
+__global__ void gather_uh_kernel(int, int, int, const int *, const double *, double *);
+__global__ void assemble_h_kernel(int, int, int, long long, const int *, const int *, const int *, const int *,
+                                  const int *, const double *, double *);
+__global__ void assemble_r_kernel(int, int, int, int, const int *, const int *, const int *, const double *, double *);
+__global__ void bsr_matvec_kernel(int, int, const long long *, const int *, const double *, const double *, double *);
+template <int NT>
+__global__ void bilu0_color_kernel(int, const int *, int, const long long *, const int *, const int *, double *, int *);
+__global__ void bilu0_fwd_kernel(int, const int *, int, const long long *, const int *, const int *, const double *,
+                                 const double *, double *);
+__global__ void bilu0_bwd_kernel(int, const int *, int, const long long *, const int *, const int *, const double *,
+                                 const double *, double *);
+__global__ void backsub_kernel(int, int, int, int, const int *, const double *, const double *, const double *, double *);
+__global__ void dot_partial_kernel(size_t, const double *, const double *, double *);
+__global__ void dot_final_kernel(int, const double *, double *, int);
+__global__ void axpy_kernel(size_t, const double *, double, const double *, double *);
+__global__ void scale_div_kernel(size_t, const double *, const double *, double *);
+__global__ void sub_kernel(size_t, const double *, const double *, double *);
+__global__ void axpby_kernel(size_t, double, const double *, double, double *);
+struct GmresState {
+    double *H, *cs, *sn, *g, *y;
+    double *scal;
+};
+__global__ void givens_kernel(GmresState, int, int);
+__global__ void hess_solve_kernel(GmresState, int, int);
+__global__ void gmres_init_kernel(GmresState, int);
+
+static int sm_count() {
+    static int n = 0;
+    if (!n) { int d = 0; cudaGetDevice(&d); cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d); }
+    return n;
+}
+static unsigned grid_for(size_t n, int threads) {
+    size_t g = (n + threads - 1) / threads;
+    size_t cap = (size_t)sm_count() * 8;
+    if (g > cap) g = cap;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+static int launched() { return cudaGetLastError() == cudaSuccess ? 0 : -12; }
+
+static size_t bilu_smem(int bs) { return sizeof(double) * (4 * (size_t)bs * bs + 200 + 4 + 1); }
+
+static int matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *y, cudaStream_t st) {
+    const int threads = 256;
+    const unsigned grid = grid_for((size_t)A->nf * 32, threads);
+    bsr_matvec_kernel<<<grid, threads, 0, st>>>(A->nf, A->bs, A->rowpts, A->colind, Hg, x, y);
+    return launched();
+}
+
+static int bilu0_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *y, double *v, cudaStream_t st) {
+    const int threads = 256, warps = threads / 32;
+    for (int c = 0; c < A->ncolors; c++) {
+        const int r0 = A->color_ptr[c], nr = A->color_ptr[c + 1] - r0;
+        if (nr <= 0) continue;
+        unsigned grid = (unsigned)((nr + warps - 1) / warps);
+        bilu0_fwd_kernel<<<grid, threads, 0, st>>>(A->bs, A->color_rows + r0, nr, A->rowpts, A->colind, A->pos, Mg, x, y);
+    }
+    for (int c = A->ncolors - 1; c >= 0; c--) {
+        const int r0 = A->color_ptr[c], nr = A->color_ptr[c + 1] - r0;
+        if (nr <= 0) continue;
+        unsigned grid = (unsigned)((nr + warps - 1) / warps);
+        bilu0_bwd_kernel<<<grid, threads, sizeof(double) * warps * A->bs, st>>>(A->bs, A->color_rows + r0, nr, A->rowpts,
+                                                                                  A->colind, A->pos, Mg, y, v);
+    }
+    return launched();
+}
+
+// dot(a,b) -> *out (device); part: scratch of >= 1024 doubles
+static void dot(size_t n, const double *a, const double *b, double *out, double *part, int do_sqrt, cudaStream_t st) {
+    const int threads = 256;
+    unsigned grid = grid_for(n, threads);
+    if (grid > 1024) grid = 1024;
+    dot_partial_kernel<<<grid, threads, 0, st>>>(n, a, b, part);
+    dot_final_kernel<<<1, 256, 0, st>>>((int)grid, part, out, do_sqrt);
+}
+}  // namespace hdgx
+
+using namespace hdgx;
+
+extern "C" {
+
+int hdgx_gather_uh(int ncu, int ndf, int ne, const int *elcon, const double *UH, double *UHe, hdgx_stream_t stream) {
+    if (ne < 0 || ncu < 1 || ndf < 1) return -1;
+    if (ne == 0) return 0;
+    if (!elcon || !UH || !UHe) return -1;
+    const size_t n = (size_t)ncu * ndf * ne;
+    gather_uh_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(ncu, ndf, ne, elcon, UH, UHe);
+    return launched();
+}
+
+int hdgx_globalassembly(const hdgx_bsr *A, const hdgx_assembly_map *map, int ncu, int npf, int nfe, const int *elcon,
+                        const double *AE, const double *FE, double *Hg, double *Rg, hdgx_stream_t stream) {
+    if (!A || !map || !elcon || !AE || !FE || !Hg || !Rg) return -1;
+    if (A->bs != ncu * npf) return -2;
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned g = (unsigned)(A->nnzb < (long long)sm_count() * 64 ? A->nnzb : (long long)sm_count() * 64);
+    if (g < 1) g = 1;
+    assemble_h_kernel<<<g, 256, 0, st>>>(ncu, npf, nfe, A->nnzb, map->blk_e, map->blk_ab, map->blk_row, A->colind,
+                                         elcon, AE, Hg);
+    const size_t n = (size_t)A->bs * A->nf;
+    assemble_r_kernel<<<grid_for(n, 256), 256, 0, st>>>(ncu, npf, nfe, A->nf, map->face_e, map->face_a, elcon, FE, Rg);
+    return launched();
+}
+
+int hdgx_matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *y, hdgx_stream_t stream) {
+    if (!A || !Hg || !x || !y) return -1;
+    return matvec(A, Hg, x, y, (cudaStream_t)stream);
+}
+
+int hdgx_bilu0_factor(const hdgx_bsr *A, double *Mg, int *status, hdgx_stream_t stream) {
+    if (!A || !Mg || A->bs > 128 || A->bs < 1) return -1;
+    cudaStream_t st = (cudaStream_t)stream;
+    constexpr int NT = 256;
+    const size_t smem = bilu_smem(A->bs);
+    if (smem > 200 * 1024) return -3;
+    if (cudaFuncSetAttribute(bilu0_color_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return -10;
+    for (int c = 0; c < A->ncolors; c++) {
+        const int r0 = A->color_ptr[c], nr = A->color_ptr[c + 1] - r0;
+        if (nr <= 0) continue;
+        unsigned grid = (unsigned)(nr < sm_count() * 8 ? nr : sm_count() * 8);
+        bilu0_color_kernel<NT><<<grid, NT, smem, st>>>(A->bs, A->color_rows + r0, nr, A->rowpts, A->colind, A->pos, Mg,
+                                                       status);
+    }
+    return launched();
+}
+
+int hdgx_bilu0_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *v, double *work, hdgx_stream_t stream) {
+    if (!A || !Mg || !x || !v || !work) return -1;
+    return bilu0_apply(A, Mg, x, work, v, (cudaStream_t)stream);
+}
+
+int hdgx_backsub(int npv, int nc, int ncu, int ndf, int ne, const int *elcon, const double *DUDG,
+                 const double *DUDG_DUH, const double *DUH, double *DUDGT, hdgx_stream_t stream) {
+    if (ne < 0 || !elcon || !DUDG || !DUDG_DUH || !DUH || !DUDGT) return -1;
+    if (ne == 0) return 0;
+    const int nh = ncu * ndf;
+    unsigned g = (unsigned)(ne < sm_count() * 16 ? ne : sm_count() * 16);
+    backsub_kernel<<<g, 128, sizeof(double) * nh, (cudaStream_t)stream>>>(ne, npv * nc, ncu, ndf, elcon, DUDG, DUDG_DUH,
+                                                                          DUH, DUDGT);
+    return launched();
+}
+
+size_t hdgx_gmres_workspace_bytes(const hdgx_bsr *A, int restart) {
+    if (!A || restart < 1) return 0;
+    const size_t N = (size_t)A->bs * A->nf;
+    const size_t m = (size_t)restart;
+    return sizeof(double) * (N * (m + 1) + 3 * N + (m + 1) * m + 4 * (m + 1) + 8 + 1024) + 256;
+}
+
+int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, const double *b, double *x, int restart,
+                     double tol, int maxit, int *iters, int *flag, double *relres, double *history, void *workspace,
+                     hdgx_stream_t stream) {
+    if (!A || !Hg || !Mg || !b || !x || restart < 1 || maxit < 1) return -1;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t N = (size_t)A->bs * A->nf;
+    const int m = restart;
+    void *mem = workspace;
+    bool own = false;
+    if (!mem) {
+        if (cudaMallocAsync(&mem, hdgx_gmres_workspace_bytes(A, restart), st) != cudaSuccess) return -13;
+        own = true;
+    }
+    double *V = (double *)mem;
+    double *pb = V + N * (m + 1), *t = pb + N, *w2 = t + N;
+    GmresState gs;
+    gs.H = w2 + N;
+    gs.cs = gs.H + (size_t)(m + 1) * m;
+    gs.sn = gs.cs + (m + 1);
+    gs.g = gs.sn + (m + 1);
+    gs.y = gs.g + (m + 1);
+    gs.scal = gs.y + (m + 1);
+    double *part = gs.scal + 8;
+    double *h_nrmb = nullptr, *h_res = nullptr;
+    cudaMallocHost(&h_nrmb, sizeof(double) * 2);
+    h_res = h_nrmb + 1;
+    int rc = 0;
+    // pb = P^{-1} b, nrmb = |pb|
+    rc |= bilu0_apply(A, Mg, b, t, pb, st);
+    dot(N, pb, pb, gs.scal + 2, part, 1, st);
+    cudaMemcpyAsync(h_nrmb, gs.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    const double nrmb = *h_nrmb;
+    int iter = 0, fl = 2;
+    double res_rel = 0.0;
+    if (!(nrmb > 0.0)) { fl = 0; res_rel = 0.0; }
+    while (fl == 2) {
+        // r = pb - P^{-1} A x -> V[:,0] = r / beta
+        rc |= matvec(A, Hg, x, t, st);
+        rc |= bilu0_apply(A, Mg, t, w2, V, st);
+        sub_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, pb, V, V);
+        dot(N, V, V, gs.scal + 0, part, 1, st);
+        scale_div_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, gs.scal + 0, V, V);
+        gmres_init_kernel<<<1, 64, 0, st>>>(gs, m);
+        int jdone = 0;
+        bool stop = false;
+        for (int j = 0; j < m; j++) {
+            double *vj = V + N * j, *w = V + N * (j + 1);
+            rc |= matvec(A, Hg, vj, t, st);
+            rc |= bilu0_apply(A, Mg, t, w2, w, st);
+            double *hc = gs.H + (size_t)(m + 1) * j;
+            for (int i = 0; i <= j; i++) {            // modified Gram-Schmidt (gmres_bilu0.m:59-63)
+                dot(N, V + N * i, w, hc + i, part, 0, st);
+                axpy_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, hc + i, -1.0, V + N * i, w);
+            }
+            dot(N, w, w, hc + j + 1, part, 1, st);
+            scale_div_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, hc + j + 1, w, w);
+            givens_kernel<<<1, 1, 0, st>>>(gs, m, j);
+            cudaMemcpyAsync(h_res, gs.scal + 1, sizeof(double), cudaMemcpyDeviceToHost, st);
+            cudaStreamSynchronize(st);
+            res_rel = *h_res / nrmb;
+            if (history && iter < maxit) history[iter] = res_rel;
+            iter++;
+            jdone = j + 1;
+            if (!isfinite(res_rel)) { fl = 3; stop = true; break; }
+            if (res_rel <= tol) { fl = 0; stop = true; break; }
+            if (iter >= maxit) { fl = 1; stop = true; break; }
+        }
+        hess_solve_kernel<<<1, 1, 0, st>>>(gs, m, jdone);
+        // x += V y  (y on the device; one axpy per basis vector)
+        for (int i = 0; i < jdone; i++) axpy_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, gs.y + i, 1.0, V + N * i, x);
+        if (stop) break;
+    }
+    cudaStreamSynchronize(st);
+    if (iters) *iters = iter;
+    if (flag) *flag = fl;
+    if (relres) *relres = res_rel;
+    cudaFreeHost(h_nrmb);
+    if (own) cudaFreeAsync(mem, st);
+    if (cudaGetLastError() != cudaSuccess) return -12;
+    return rc ? -12 : 0;
+}
+
+}  // extern "C"

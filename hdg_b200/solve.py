@@ -1,0 +1,213 @@
+"""Newton solve of a steady HDG problem on the GPU (the reference's hdg_solve call surface).
+
+``hdg_solve(master, mesh, app, UDG, UH, SH)`` follows kernel/hdg_solve.m:104-176:
+  assemble (elemental kernel + block-CSR global assembly) -> F, K, DUDG, DUDG_DUH
+  while |F|/|F0| > tol and it < maxiter:
+      DUH   = K \\ F           (BILU(0)-preconditioned GMRES on the GPU; the reference's
+                               default is a sparse direct K\\F, hdg_solve.m:111)
+      DUDGT = DUDG + DUDG_DUH DUH(elcon)                      (hdg_solve.m:119-121)
+      damped update UDG += alfa DUDGT, UH += alfa DUH with alfa halved while |F| grows
+      (hdg_solve.m:139-163)
+Everything stays resident on the device across iterations; only scalars come back.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from ._lib import HdgxAssemblyMap, HdgxBsr, check, lib
+from .elemental import (DArray, DeviceMaster, alloc_elemental_outputs, app_struct, as_darray, _require_cuda,
+                        _stream_ptr)
+from .ordering import assembly_map, multicolor
+
+
+class TraceSystem:
+    """Device-resident block-CSR pattern, elimination order and assembly map of a mesh."""
+
+    def __init__(self, mesh, master, app, ordering=None):
+        _require_cuda()
+        self.nf, self.npf, self.nfe, self.ncu = mesh.nf, master.npf, master.nfe, app.ncu
+        self.bs = app.ncu * master.npf
+        self.nnzb = int(mesh.cbsr_rowpts[-1])
+        self.ord = ordering if ordering is not None else multicolor(mesh.cbsr_rowpts, mesh.cbsr_colind, mesh.nf)
+        am = assembly_map(mesh.t2f, mesh.cbsr_rowpts, mesh.cbsr_colind)
+        i32 = torch.int32
+        self.d = dict(
+            rowpts=DArray.from_numpy(np.asarray(mesh.cbsr_rowpts, dtype=np.int64), dtype=torch.int64),
+            colind=DArray.from_numpy(mesh.cbsr_colind, dtype=i32),
+            color_rows=DArray.from_numpy(self.ord.color_rows, dtype=i32),
+            pos=DArray.from_numpy(self.ord.pos, dtype=i32),
+            blk_e=DArray.from_numpy(am.blk_e, dtype=i32), blk_ab=DArray.from_numpy(am.blk_ab, dtype=i32),
+            blk_row=DArray.from_numpy(am.blk_row, dtype=i32), face_e=DArray.from_numpy(am.face_e, dtype=i32),
+            face_a=DArray.from_numpy(am.face_a, dtype=i32), elcon=DArray.from_numpy(mesh.elcon, dtype=i32))
+        self.color_ptr = np.ascontiguousarray(self.ord.color_ptr, dtype=np.int32)
+        d = self.d
+        self.bsr = HdgxBsr(self.nf, self.bs, self.nnzb, d["rowpts"].ptr, d["colind"].ptr, self.ord.ncolors,
+                           self.color_ptr.ctypes.data, d["color_rows"].ptr, d["pos"].ptr)
+        self.map = HdgxAssemblyMap(d["blk_e"].ptr, d["blk_ab"].ptr, d["blk_row"].ptr, d["face_e"].ptr,
+                                   d["face_a"].ptr)
+
+    def empty_blocks(self):
+        return DArray.empty((self.bs, self.bs, self.nnzb))
+
+    def empty_vec(self):
+        return DArray.empty((self.bs, self.nf))
+
+    # ------------------------------------------------------------ operations
+    def assemble(self, AE, FE, Hg, Rg, stream=None):
+        rc = lib().hdgx_globalassembly(ct.byref(self.bsr), ct.byref(self.map), self.ncu, self.npf, self.nfe,
+                                       self.d["elcon"].ptr, AE.ptr, FE.ptr, Hg.ptr, Rg.ptr, _stream_ptr(stream))
+        check(rc, "hdgx_globalassembly")
+
+    def matvec(self, Hg, x, y, stream=None):
+        check(lib().hdgx_matvec(ct.byref(self.bsr), Hg.ptr, x.ptr, y.ptr, _stream_ptr(stream)), "hdgx_matvec")
+
+    def bilu0(self, Hg, Mg, status=None, stream=None):
+        Mg.t.copy_(Hg.t)
+        st = status.ptr if status is not None else None
+        check(lib().hdgx_bilu0_factor(ct.byref(self.bsr), Mg.ptr, st, _stream_ptr(stream)), "hdgx_bilu0_factor")
+
+    def bilu0_apply(self, Mg, x, v, work, stream=None):
+        check(lib().hdgx_bilu0_apply(ct.byref(self.bsr), Mg.ptr, x.ptr, v.ptr, work.ptr, _stream_ptr(stream)),
+              "hdgx_bilu0_apply")
+
+    def gmres(self, Hg, Mg, b, x, restart=20, tol=1e-10, maxit=1000, workspace=None, stream=None):
+        it, fl, rr = ct.c_int(0), ct.c_int(0), ct.c_double(0.0)
+        hist = np.zeros(maxit + 1)
+        ws = workspace.data_ptr() if workspace is not None else None
+        rc = lib().hdgx_gmres_bilu0(ct.byref(self.bsr), Hg.ptr, Mg.ptr, b.ptr, x.ptr, int(restart), float(tol),
+                                    int(maxit), ct.byref(it), ct.byref(fl), ct.byref(rr),
+                                    hist.ctypes.data_as(ct.c_void_p), ws, _stream_ptr(stream))
+        check(rc, "hdgx_gmres_bilu0")
+        return it.value, fl.value, rr.value, hist[:it.value]
+
+    def workspace(self, restart):
+        nb = lib().hdgx_gmres_workspace_bytes(ct.byref(self.bsr), int(restart))
+        return torch.empty(int(nb), dtype=torch.uint8, device="cuda")
+
+
+@dataclass
+class SolveReport:
+    iterations: int = 0
+    residuals: list = field(default_factory=list)       # |F| after every Newton step (F0 first)
+    alphas: list = field(default_factory=list)
+    gmres_iters: list = field(default_factory=list)
+    gmres_relres: list = field(default_factory=list)
+    times: dict = field(default_factory=dict)
+    converged: bool = False
+
+
+class HDGSolver:
+    """Device-resident state of one steady problem (mesh, master, app) for Newton steps."""
+
+    def __init__(self, master, mesh, app, ordering=None, restart=20):
+        _require_cuda()
+        self.master, self.mesh, self.app = master, mesh, app
+        self.dm = DeviceMaster(master)
+        self.ts = TraceSystem(mesh, master, app, ordering)
+        ne = mesh.ne
+        self.ne = ne
+        self.dg = DArray.from_numpy(mesh.dgnodes)
+        self.bf = DArray.from_numpy(mesh.bf, dtype=torch.int32)
+        self.out = alloc_elemental_outputs(master, app, ne)
+        self.Hg = self.ts.empty_blocks()
+        self.Mg = self.ts.empty_blocks()
+        self.Rg = self.ts.empty_vec()
+        self.DUH = self.ts.empty_vec()
+        self.work = self.ts.empty_vec()
+        ndf = master.npf * master.nfe
+        self.UHe = DArray.empty((app.ncu, ndf, ne))
+        self.DUDGT = DArray.empty((master.npv, app.nc, ne))
+        self.app_c = app_struct(app)
+        self.restart = restart
+        self.ws = self.ts.workspace(restart)
+
+    def gather(self, UH, stream=None):
+        ndf = self.master.npf * self.master.nfe
+        check(lib().hdgx_gather_uh(self.app.ncu, ndf, self.ne, self.ts.d["elcon"].ptr, UH.ptr, self.UHe.ptr,
+                                   _stream_ptr(stream)), "hdgx_gather_uh")
+
+    def assemble(self, UDG, UH, SH, stream=None):
+        """hdg_assemble: elemental kernel + global assembly; returns |F|."""
+        self.gather(UH, stream)
+        L = lib()
+        o = self.out
+        rc = L.hdgx_elemental(ct.byref(self.dm.c), ct.byref(self.app_c), self.ne, self.dg.ptr, self.bf.ptr, UDG.ptr,
+                              self.UHe.ptr, SH.ptr, o.AE.ptr, o.FE.ptr, o.DUDG.ptr, o.DUDG_DUH.ptr, o.status.ptr,
+                              _stream_ptr(stream))
+        check(rc, "hdgx_elemental")
+        self.ts.assemble(o.AE, o.FE, self.Hg, self.Rg, stream)
+        return float(torch.linalg.vector_norm(self.Rg.t).item())
+
+    def linear_solve(self, tol=1e-10, maxit=1000, stream=None):
+        """DUH = K \\ F with BILU(0)-GMRES (x0 = 0)."""
+        self.ts.bilu0(self.Hg, self.Mg, stream=stream)
+        self.DUH.t.zero_()
+        return self.ts.gmres(self.Hg, self.Mg, self.Rg, self.DUH, self.restart, tol, maxit, self.ws, stream)
+
+    def backsub(self, stream=None):
+        m, a = self.master, self.app
+        ndf = m.npf * m.nfe
+        o = self.out
+        check(lib().hdgx_backsub(m.npv, a.nc, a.ncu, ndf, self.ne, self.ts.d["elcon"].ptr, o.DUDG.ptr,
+                                 o.DUDG_DUH.ptr, self.DUH.ptr, self.DUDGT.ptr, _stream_ptr(stream)), "hdgx_backsub")
+
+    def solve(self, UDG, UH, SH, tol=1e-10, maxiter=16, gmres_tol=1e-10, gmres_maxit=1000, linear=False):
+        """The Newton loop of hdg_solve.m; UDG [npv,nc,ne], UH [ncu,nsiz] device arrays (updated)."""
+        rep = SolveReport()
+        t0 = time.perf_counter()
+        F = self.assemble(UDG, UH, SH)
+        F0 = F
+        rep.residuals.append(F)
+        rel = 1.0
+        it = 0
+        UDG0 = torch.empty_like(UDG.t)
+        UH0 = torch.empty_like(UH.t)
+        while rel > tol and it < maxiter:
+            gi, gf, grr, _ = self.linear_solve(gmres_tol, gmres_maxit)
+            rep.gmres_iters.append(gi)
+            rep.gmres_relres.append(grr)
+            self.backsub()
+            if linear:
+                UDG.t.add_(self.DUDGT.t)
+                UH.t.add_(self.DUH.t.view(-1))
+                rep.iterations = 1
+                return rep
+            it += 1
+            UDG0.copy_(UDG.t)
+            UH0.copy_(UH.t)
+            duh0 = F
+            alfa = 1.0
+            while True:
+                torch.add(UDG0, self.DUDGT.t, alpha=alfa, out=UDG.t)
+                torch.add(UH0, self.DUH.t.view(-1), alpha=alfa, out=UH.t)
+                F = self.assemble(UDG, UH, SH)
+                if F > duh0:
+                    alfa /= 2
+                    if alfa < 1e-2:
+                        break
+                else:
+                    break
+            rep.alphas.append(alfa)
+            rep.residuals.append(F)
+            rel = F / F0 if F0 > 0 else 0.0
+        torch.cuda.synchronize()
+        rep.iterations = it
+        rep.converged = rel <= tol
+        rep.times["total_s"] = time.perf_counter() - t0
+        return rep
+
+
+def hdg_solve(master, mesh, app, UDG, UH, SH=None, tol=1e-10, maxiter=16, gmres_tol=1e-10, restart=20,
+              ordering=None):
+    """kernel/hdg_solve.m: returns (UDG, UH, report) as host arrays (inputs are not modified)."""
+    s = HDGSolver(master, mesh, app, ordering=ordering, restart=restart)
+    dU = DArray.from_numpy(UDG)
+    dH = DArray.from_numpy(UH)
+    dS = DArray.from_numpy(np.zeros_like(UDG) if SH is None else SH)
+    rep = s.solve(dU, dH, dS, tol=tol, maxiter=maxiter, gmres_tol=gmres_tol)
+    return dU.numpy(), dH.numpy(), rep

@@ -26,6 +26,7 @@
 #ifndef HDGX_H
 #define HDGX_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -97,6 +98,71 @@ int hdgx_schur_u(int npv, int ncu, int nc, int ndf, int ne,
                  const double *BD, const double *F, const double *GK, const double *H,
                  const double *Ru, const double *Rh, double *DUDG, double *DUDG_DUH,
                  double *AE, double *FE, int *status, hdgx_stream_t stream);
+
+/* ---------------------------------------------------------------- trace system */
+
+/* Face-row block-CSR pattern of the condensed system (mesh.cbsr_* of block_crs.m) and the
+ * elimination order used by BILU(0).  Block size bs = ncu*npf.  Device pointers except
+ * color_ptr (host).  Rows are eliminated colour by colour; rows of one colour share no
+ * block, pos[row] is the row's position in the elimination order. */
+typedef struct {
+    int nf, bs;
+    long long nnzb;
+    const long long *rowpts;   /* [nf+1] block offsets, 0-based */
+    const int *colind;         /* [nnzb] 1-based block column, diagonal first in each row */
+    int ncolors;
+    const int *color_ptr;      /* HOST [ncolors+1] offsets into color_rows */
+    const int *color_rows;     /* [nf] 0-based rows grouped by colour */
+    const int *pos;            /* [nf] elimination position of each row */
+} hdgx_bsr;
+
+/* Element -> block gather map for hdgx_globalassembly (device pointers):
+ * blk_e[2*nnzb] elements (or -1) contributing to block k, blk_ab[2*nnzb] their local
+ * faces (a | b << 8), blk_row[nnzb] 0-based block row; face_e[2*nf], face_a[2*nf] the
+ * (element, local face) pairs of every face (element -1 when absent). */
+typedef struct {
+    const int *blk_e, *blk_ab, *blk_row;
+    const int *face_e, *face_a;
+} hdgx_assembly_map;
+
+/* UHe[ncu, ndf, ne] = UH[:, elcon] (kernel/hdg_assemble.m:34).  elcon [ndf, ne] 1-based. */
+int hdgx_gather_uh(int ncu, int ndf, int ne, const int *elcon, const double *UH, double *UHe,
+                   hdgx_stream_t stream);
+
+/* Hg[bs,bs,nnzb], Rg[bs,nf] from AE[ncu,ndf,ncu,ndf,ne], FE[ncu,ndf,ne]
+ * (kernel/globalassembly.m:21-37; dofs placed by elcon as kernel/hdg_assemble.m:77-87). */
+int hdgx_globalassembly(const hdgx_bsr *A, const hdgx_assembly_map *map, int ncu, int npf, int nfe,
+                        const int *elcon, const double *AE, const double *FE, double *Hg, double *Rg,
+                        hdgx_stream_t stream);
+
+/* y = Hg x (kernel/matvec.m). */
+int hdgx_matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *y, hdgx_stream_t stream);
+
+/* In-place block ILU(0) of Mg (= Hg on entry) in the colour order of A
+ * (kernel/computeBILU0.m); diagonal blocks are stored inverted.  status[nf] (optional) is
+ * set to 1 for rows whose pivot block is singular. */
+int hdgx_bilu0_factor(const hdgx_bsr *A, double *Mg, int *status, hdgx_stream_t stream);
+
+/* v = (L U)^{-1} x (kernel/applyBILU0.m); work[bs*nf] scratch. */
+int hdgx_bilu0_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *v, double *work,
+                     hdgx_stream_t stream);
+
+/* Bytes of device workspace hdgx_gmres_bilu0 uses for a given restart length. */
+size_t hdgx_gmres_workspace_bytes(const hdgx_bsr *A, int restart);
+
+/* Left-preconditioned restarted GMRES with modified Gram-Schmidt (kernel/gmres_bilu0.m):
+ * x (in: initial guess, out: solution) [bs,nf]; stops when |P^{-1}(b - A x)| <= tol |P^{-1} b|
+ * or after maxit iterations.  iters, flag (0 converged, 1 maxit, 3 breakdown), relres and
+ * history[maxit] (optional) are host outputs.  workspace (device, hdgx_gmres_workspace_bytes)
+ * may be NULL, in which case it is taken from the stream-ordered allocator. */
+int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, const double *b, double *x,
+                     int restart, double tol, int maxit, int *iters, int *flag, double *relres,
+                     double *history, void *workspace, hdgx_stream_t stream);
+
+/* DUDGT[npv,nc,ne] = DUDG + DUDG_DUH * DUH(:, elcon(:,e)) (kernel/hdg_solve.m:119-121);
+ * DUH[ncu, nsiz]. */
+int hdgx_backsub(int npv, int nc, int ncu, int ndf, int ne, const int *elcon, const double *DUDG,
+                 const double *DUDG_DUH, const double *DUH, double *DUDGT, hdgx_stream_t stream);
 
 #ifdef __cplusplus
 }

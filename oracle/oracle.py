@@ -177,3 +177,138 @@ def ref_fhat(nd, param, nl, udg, uh, family="ns"):
     fn(_p(fh), _p(fhu), _p(fhh), _p(pg), _p(_f(udg)), _p(_f(uh)), _p(_f(nl)), _p(_f(param)),
        ct.c_double(0.0), ng, nc, ncu, nd, nd)
     return fh, fhu, fhh
+
+
+# ------------------------------------------------------------- condensed system (CPU)
+_lp = ct.POINTER(ct.c_longlong)
+
+
+def _i32(a):
+    return np.ascontiguousarray(np.asarray(a).ravel(order="F"), dtype=np.int32)
+
+
+def _i64(a):
+    return np.ascontiguousarray(np.asarray(a).ravel(order="F"), dtype=np.int64)
+
+
+def globalassembly(mesh, AE, FE, npf, ncu):
+    """kernel/globalassembly.m: block-CSR Hg[bs,bs,nnzb], Rg[bs,nf]."""
+    L = lib()
+    ne, nfe = mesh.t2f.shape
+    bs = ncu * npf
+    nnzb = int(mesh.cbsr_rowpts[-1])
+    Hg = np.zeros((bs, bs, nnzb), order="F"); Rg = np.zeros((bs, mesh.nf), order="F")
+    t2f, el, rp, ci = _i32(mesh.t2f), _i32(mesh.elcon), _i64(mesh.cbsr_rowpts), _i32(mesh.cbsr_colind)
+    L.orc_globalassembly(ne, nfe, npf, ncu, t2f.ctypes.data_as(_ip), el.ctypes.data_as(_ip), mesh.nf,
+                         rp.ctypes.data_as(_lp), ci.ctypes.data_as(_ip), _p(_f(AE)), _p(_f(FE)), _p(Hg), _p(Rg))
+    return Hg, Rg
+
+
+def matvec(mesh, Hg, x):
+    L = lib(); bs = Hg.shape[0]
+    rp, ci = _i64(mesh.cbsr_rowpts), _i32(mesh.cbsr_colind)
+    y = np.zeros((bs, mesh.nf), order="F")
+    L.orc_matvec(mesh.nf, bs, rp.ctypes.data_as(_lp), ci.ctypes.data_as(_ip), _p(_f(Hg)), _p(_f(x)), _p(y))
+    return y
+
+
+def mdf_ordering(mesh, Hg):
+    """kernel/computeMDFordering.m -> (ordered2unordered, unordered2ordered), 0-based."""
+    L = lib(); bs = Hg.shape[0]
+    rp, ci = _i64(mesh.cbsr_rowpts), _i32(mesh.cbsr_colind)
+    o2u = np.zeros(mesh.nf, dtype=np.int32); u2o = np.zeros(mesh.nf, dtype=np.int32)
+    L.orc_mdf_ordering(mesh.nf, bs, rp.ctypes.data_as(_lp), ci.ctypes.data_as(_ip), _p(_f(Hg)),
+                       o2u.ctypes.data_as(_ip), u2o.ctypes.data_as(_ip))
+    return o2u, u2o
+
+
+def bilu0(mesh, Hg, o2u, u2o):
+    """kernel/computeBILU0.m with the given ordering; returns (Mg, status)."""
+    L = lib(); bs = Hg.shape[0]
+    rp, ci = _i64(mesh.cbsr_rowpts), _i32(mesh.cbsr_colind)
+    Mg = np.array(Hg, dtype=np.float64, order="F", copy=True)
+    rc = L.orc_bilu0(mesh.nf, bs, rp.ctypes.data_as(_lp), ci.ctypes.data_as(_ip), _i32(o2u).ctypes.data_as(_ip),
+                     _i32(u2o).ctypes.data_as(_ip), _p(Mg))
+    return Mg, rc
+
+
+def bilu0_apply(mesh, Mg, x, o2u, u2o):
+    L = lib(); bs = Mg.shape[0]
+    rp, ci = _i64(mesh.cbsr_rowpts), _i32(mesh.cbsr_colind)
+    v = np.zeros((bs, mesh.nf), order="F")
+    L.orc_bilu0_apply(mesh.nf, bs, rp.ctypes.data_as(_lp), ci.ctypes.data_as(_ip), _i32(o2u).ctypes.data_as(_ip),
+                      _i32(u2o).ctypes.data_as(_ip), _p(_f(Mg)), _p(_f(x)), _p(v))
+    return v
+
+
+def gmres_bilu0(mesh, Mg, Hg, b, x0, o2u, u2o, restart=20, tol=1e-10, maxit=1000):
+    """kernel/gmres_bilu0.m -> (x, flag, iter, rev)."""
+    L = lib(); bs = Hg.shape[0]
+    rp, ci = _i64(mesh.cbsr_rowpts), _i32(mesh.cbsr_colind)
+    x = np.array(x0, dtype=np.float64, order="F", copy=True)
+    flag = ct.c_int(0); rev = np.zeros(maxit + 1)
+    it = L.orc_gmres_bilu0(mesh.nf, bs, rp.ctypes.data_as(_lp), ci.ctypes.data_as(_ip), _i32(o2u).ctypes.data_as(_ip),
+                           _i32(u2o).ctypes.data_as(_ip), _p(_f(Mg)), _p(_f(Hg)), _p(_f(b)), _p(x), int(restart),
+                           ct.c_double(tol), int(maxit), ct.byref(flag), _p(rev))
+    return x, flag.value, it, rev[:it]
+
+
+def backsub(mesh, DUDG, DUDG_DUH, DUH):
+    """hdg_solve.m:119-121 on the CPU."""
+    L = lib()
+    npv, nc, ne = DUDG.shape
+    ncu, ndf = DUDG_DUH.shape[2], DUDG_DUH.shape[3]
+    out = np.zeros((npv, nc, ne), order="F")
+    L.orc_backsub(ne, npv, nc, ncu, ndf, _i32(mesh.elcon).ctypes.data_as(_ip), _p(_f(DUDG)), _p(_f(DUDG_DUH)),
+                  _p(_f(DUH)), _p(out))
+    return out
+
+
+def hdg_solve(P, o2u=None, u2o=None, tol=1e-10, maxiter=16, gmres_tol=1e-10, restart=20, nthreads=1):
+    """kernel/hdg_solve.m:104-176 on the CPU (oracle elemental + globalassembly + BILU(0)
+    ordered by o2u (MDF when None) + GMRES + back-substitution + damped line search).
+    Returns (UDG, UH, residuals, gmres_iters, alphas)."""
+    m, a, mesh = P.master, P.app, P.mesh
+    npf, ncu = m.npf, a.ncu
+    UDG = np.array(P.UDG, order="F", copy=True)
+    UH = np.array(P.UH, order="F", copy=True)
+
+    def assemble(UDG, UH):
+        from hdg_b200.app import gather_uh
+        r = hdg_elemental(m, a, mesh.dgnodes, mesh.bf, UDG, gather_uh(UH, mesh.elcon), P.SH, nthreads=nthreads)
+        Hg, Rg = globalassembly(mesh, r["AE"], r["FE"], npf, ncu)
+        return r, Hg, Rg
+
+    r, Hg, Rg = assemble(UDG, UH)
+    F0 = float(np.linalg.norm(Rg))
+    res, gits, alphas = [F0], [], []
+    F = F0
+    rel, it = 1.0, 0
+    while rel > tol and it < maxiter:
+        if o2u is None:
+            oo, uu = mdf_ordering(mesh, Hg)
+        else:
+            oo, uu = o2u, u2o
+        Mg, _ = bilu0(mesh, Hg, oo, uu)
+        DUH, flag, gi, _ = gmres_bilu0(mesh, Mg, Hg, Rg, np.zeros_like(Rg), oo, uu, restart, gmres_tol, 1000)
+        gits.append(gi)
+        DUH = DUH.reshape(ncu, mesh.nsiz, order="F")
+        DUDGT = backsub(mesh, r["DUDG"], r["DUDG_DUH"], DUH)
+        it += 1
+        UDG0, UH0, duh0 = UDG.copy(), UH.copy(), F
+        alfa = 1.0
+        while True:
+            UDG = UDG0 + alfa * DUDGT
+            UH = UH0 + alfa * DUH
+            r, Hg, Rg = assemble(UDG, UH)
+            F = float(np.linalg.norm(Rg))
+            if F > duh0:
+                alfa /= 2
+                if alfa < 1e-2:
+                    break
+            else:
+                break
+        alphas.append(alfa)
+        res.append(F)
+        rel = F / F0
+    return UDG, UH, res, gits, alphas

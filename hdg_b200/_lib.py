@@ -88,6 +88,8 @@ def _declare(L):
     L.hdgx_gmres_workspace_bytes.argtypes = [B, i]
     L.hdgx_gmres_bilu0.restype = i
     L.hdgx_gmres_bilu0.argtypes = [B, v, v, v, v, i, d, i, p(i), p(i), p(d), v, v, v]
+    L.hdgx_gmres_bilu0_noalloc.restype = i
+    L.hdgx_gmres_bilu0_noalloc.argtypes = [B, v, v, v, v, i, d, i, p(i), p(i), p(d), v, v]
     L.hdgx_backsub.restype = i
     L.hdgx_backsub.argtypes = [i, i, i, i, i, v, v, v, v, v, v]
     _declare_optional(L)

@@ -31,6 +31,7 @@ const char *hdgx_status_str(int code) {
         case -2: return "inconsistent dimensions (nd, ncu, nc, npv, npf, nfe)";
         case -3: return "unsupported element size (shared-memory plan does not fit)";
         case -4: return "too many boundary indices";
+        case -5: return "system too large for the allocation-free scratch (hdgx_gmres_bilu0_noalloc: 16 MiB)";
         case -10: return "cudaFuncSetAttribute failed";
         case -11: return "kernel does not fit on an SM";
         case -12: return "kernel launch failed";

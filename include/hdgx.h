@@ -159,6 +159,20 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
                      int restart, double tol, int maxit, int *iters, int *flag, double *relres,
                      double *history, void *workspace, hdgx_stream_t stream);
 
+/* Allocation-free variant of hdgx_gmres_bilu0 (same arguments minus the workspace; same
+ * algorithm and results).  No counterpart in the reference: it exists for callers that may
+ * not allocate device or pinned host memory at solve time (a plugin host whose allocator
+ * owns every byte, a latency-critical serving loop, memory already reserved in arenas).
+ * Its scratch is one 16 MiB array compiled into the library, held by every GPU that loads
+ * the library until exit; systems needing more (hdgx_gmres_workspace_bytes > 16 MiB,
+ * roughly N > 88,000 unknowns at restart 20) are rejected with status -5.  All calls share
+ * that array and it keeps the last call's contents, so calls that overlap on the GPU race;
+ * the first call on each device resolves the array's address and should come before any
+ * stream capture. */
+int hdgx_gmres_bilu0_noalloc(const hdgx_bsr *A, const double *Hg, const double *Mg, const double *b,
+                             double *x, int restart, double tol, int maxit, int *iters, int *flag,
+                             double *relres, double *history, hdgx_stream_t stream);
+
 /* DUDGT[npv,nc,ne] = DUDG + DUDG_DUH * DUH(:, elcon(:,e)) (kernel/hdg_solve.m:119-121);
  * DUH[ncu, nsiz]. */
 int hdgx_backsub(int npv, int nc, int ncu, int ndf, int ne, const int *elcon, const double *DUDG,

@@ -96,22 +96,27 @@ struct Plan {
     static constexpr int x_end = x_ZFr + (VISC ? D::NGT * D::NCU * D::ND : 0);
     static constexpr int x_size = x_end - p_end;
     // column tiles of DUDG_DUH (reuse the scratch)
-    static constexpr int per_col = D::NQ + D::NGT * D::NC + D::NGT * D::NCU;
+    static constexpr int NCG = VISC ? D::NC : D::NCU;
+    static constexpr int per_col = D::NQ + D::NGT * NCG + D::NGT * D::NCU;
     static constexpr int TILE_RAW = x_size / per_col;
     static constexpr int TILE = TILE_RAW < 1 ? 1 : (TILE_RAW > D::NH ? D::NH : TILE_RAW);
     static constexpr int y_X = p_end;
     static constexpr int y_Xg = y_X + D::NQ * TILE;
-    static constexpr int y_Y = y_Xg + D::NGT * D::NC * TILE;
+    static constexpr int y_Y = y_Xg + D::NGT * NCG * TILE;
     static constexpr int y_end = y_Y + D::NGT * D::NCU * TILE;
     static constexpr int d_slots = (x_end > y_end ? x_end : y_end);   // 3 x u64 pivot slots
-    static constexpr int n_doubles = d_slots + 4;
+    static constexpr int d_pcol = d_slots + 4;                          // [4*NU] pivot column copies
+    static constexpr int d_diag = d_pcol + 4 * D::NU;                   // [NU] pivots
+    static constexpr int n_doubles = d_diag + D::NU;
     // integers after the doubles
     static constexpr int i_perm = 0;                      // [NPF, NFE] 0-based
     static constexpr int i_invp = D::NPF * D::NFE;        // [NPV, NFE] face-local index or -1
     static constexpr int i_piv = i_invp + D::NPV * D::NFE;
     static constexpr int i_pivM = i_piv + D::NU;
     static constexpr int i_rowused = i_pivM + D::NPV;
-    static constexpr int i_bf = i_rowused + D::NU;
+    static constexpr int i_rowvar = i_rowused + D::NU;
+    static constexpr int i_gslot = i_rowvar + D::NU;
+    static constexpr int i_bf = i_gslot + 2;
     static constexpr int i_bad = i_bf + D::NFE;
     static constexpr int n_ints = i_bad + 1;
     static constexpr size_t bytes = sizeof(double) * n_doubles + sizeof(int) * n_ints;
@@ -127,6 +132,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
     constexpr int NFE = D::NFE, NCU = D::NCU, NC = D::NC, NDF = D::NDF, NU = D::NU;
     constexpr int NQ = D::NQ, NH = D::NH, NGT = D::NGT;
     constexpr int NSEED = VISC ? NC : NCU;   // inviscid flux does not depend on q
+    constexpr int NCG = VISC ? NC : NCU;     // components dRh/dudg couples (q-part is 0 for Euler)
     extern __shared__ __align__(16) double sm[];
     int *si = reinterpret_cast<int *>(sm + L::n_doubles);
     const int tid = threadIdx.x;
@@ -167,8 +173,9 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
     double *x_Zc = sm + L::x_Zc, *x_Ze = sm + L::x_Ze, *x_Zr = sm + L::x_Zr;
     double *x_ZFc = sm + L::x_ZFc, *x_ZFe = sm + L::x_ZFe, *x_ZFr = sm + L::x_ZFr;
     int *s_piv = si + L::i_piv, *s_pivM = si + L::i_pivM, *s_bf = si + L::i_bf, *s_bad = si + L::i_bad;
-    int *s_rowused = si + L::i_rowused;
+    int *s_rowused = si + L::i_rowused, *s_rowvar = si + L::i_rowvar, *s_gslot = si + L::i_gslot;
     unsigned long long *s_slot = reinterpret_cast<unsigned long long *>(sm + L::d_slots);
+    double *s_pcol = sm + L::d_pcol, *s_diag = sm + L::d_diag;
 
     for (int e = blockIdx.x; e < P.ne; e += gridDim.x) {
         // ================================================================ load
@@ -324,8 +331,8 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
 
         // ============================ Mi = inv(M): MiC, MiE, MiRq (schur_primal.m:86-91)
         // M is SPD (exact quadrature of phi phi jac): eliminate without pivoting
-        block_gauss_jordan<NT, false>(s_M, NPV, s_MiC, NPV, NPV, NPV * ND + NDF * ND + NCU * ND,
-                                      s_pivM, s_rowused, s_slot, s_bad);
+        gj_regs<NPV, NPV * ND + NDF * ND + NCU * ND, NT, 8, false>(s_M, s_MiC, s_pcol, s_diag, s_rowvar,
+                                                                  s_gslot, s_bad);
         if (tid == 0 && *s_bad) *s_bad = 1;
         __syncthreads();
 
@@ -571,7 +578,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
         {
             int bad_before = *s_bad;
             __syncthreads();
-            block_gauss_jordan<NT, true>(s_SD, NU, s_R, NU, NU, 1 + NH, s_piv, s_rowused, s_slot, s_bad);
+            gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
             if (tid == 0 && *s_bad && !bad_before) *s_bad = 2;
             __syncthreads();
         }
@@ -583,12 +590,12 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
                 const int r = i % NPV, c = i / NPV;
                 double v;
                 if (c < NCU) {
-                    v = s_R[s_piv[r + NPV * c]];
+                    v = s_R[r + NPV * c];
                 } else {
                     const int a = (c - NCU) % NCU, d = (c - NCU) / NCU;
                     v = s_MiRq[r + NPV * (a + NCU * d)];
 #pragma unroll
-                    for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * s_R[s_piv[s + NPV * a]];
+                    for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * s_R[s + NPV * a];
                 }
                 s_dudg[i] = v;
                 g_dudg[i] = v;
@@ -598,7 +605,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
         // FE = Rh - GK DUDG (schur_primal.m:143-144), GK applied at the face Gauss points
         {
             double *Xg = sm + L::y_Xg;
-            for (int i = tid; i < NGT * NC; i += NT) {
+            for (int i = tid; i < NGT * NCG; i += NT) {
                 const int gg = i % NGT, c = i / NGT, g = gg % NGF, j = gg / NGF;
                 double t = 0.0;
 #pragma unroll
@@ -613,7 +620,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
                 for (int g = 0; g < NGF; g++) {
                     const int gg = g + NGF * j;
                     double y = 0.0;
-                    for (int c = 0; c < NC; c++) y += s_Gp[gg + NGT * (a + NCU * c)] * Xg[gg + NGT * c];
+                    for (int c = 0; c < NCG; c++) y += s_Gp[gg + NGT * (a + NCU * c)] * Xg[gg + NGT * c];
                     t += t_fg[n + NPF * g] * y;
                 }
                 g_fe[i] = s_Rh[i] - t;
@@ -635,20 +642,20 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
                     const double *dlu = s_R + NU * (1 + k);
                     double v;
                     if (c < NCU) {
-                        v = dlu[s_piv[r + NPV * c]];
+                        v = dlu[r + NPV * c];
                     } else {
                         const int a = (c - NCU) % NCU, d = (c - NCU) / NCU;
                         const int b = k % NCU, f = k / NCU;
                         v = (a == b) ? -s_MiE[r + NPV * (f + NDF * d)] : 0.0;
 #pragma unroll
-                        for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * dlu[s_piv[s + NPV * a]];
+                        for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * dlu[s + NPV * a];
                     }
                     yX[i] = v;
                     g_dd[(size_t)NQ * k0 + i] = v;
                 }
                 __syncthreads();
-                for (int i = tid; i < NGT * NC * nt; i += NT) {
-                    const int gg = i % NGT, c = (i / NGT) % NC, t = i / (NGT * NC);
+                for (int i = tid; i < NGT * NCG * nt; i += NT) {
+                    const int gg = i % NGT, c = (i / NGT) % NCG, t = i / (NGT * NCG);
                     const int g = gg % NGF, j = gg / NGF;
                     double v = 0.0;
 #pragma unroll
@@ -659,7 +666,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
                 for (int i = tid; i < NGT * NCU * nt; i += NT) {
                     const int gg = i % NGT, a = (i / NGT) % NCU, t = i / (NGT * NCU);
                     double v = 0.0;
-                    for (int c = 0; c < NC; c++) v += s_Gp[gg + NGT * (a + NCU * c)] * yXg[gg + NGT * (c + NC * t)];
+                    for (int c = 0; c < NCG; c++) v += s_Gp[gg + NGT * (a + NCU * c)] * yXg[gg + NGT * (c + NCG * t)];
                     yY[i] = v;
                 }
                 __syncthreads();

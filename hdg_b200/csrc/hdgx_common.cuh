@@ -247,4 +247,115 @@ __device__ void block_gauss_jordan(double *A, int lda, double *B, int ldb, int n
     __syncthreads();
 }
 
+// Gauss-Jordan elimination of the augmented system [A | B] (A: N x N, B: N x NR, both
+// column-major with leading dimension N, in shared memory) with the matrix held in
+// REGISTERS: thread (tr, tc) = (tid % TR, tid / TR) owns rows tr + i*TR and columns
+// tc + jj*TC of the augmented matrix.  Per step k: the pivot row is broadcast inside each
+// TR-lane group with __shfl_sync, the multipliers come from a shared copy of column k that
+// the owners of column k wrote at the end of step k-1, and the owners also picked the
+// step-k pivot there (max |value| over the rows not yet used, reduced with shuffles inside
+// their TR-lane group), so one barrier per step suffices.  On return B holds the solution in natural row
+// order.  PIVOT = false eliminates in natural order (SPD matrices).  *bad = k+1 for the
+// first zero or non-finite pivot.  Shared scratch: pcol[2N] (column copy, double-buffered),
+// diag[N], rowvar[N] (ints), slot[2] (ints).
+template <int N, int NR, int NT, int TR, bool PIVOT>
+__device__ __forceinline__ void gj_regs(const double *__restrict__ A, double *B, double *pcol, double *diag,
+                                        int *rowvar, int *slot, int *bad) {
+    static_assert(32 % TR == 0 && NT % TR == 0, "TR must divide 32 and NT");
+    constexpr int NCOL = N + NR;
+    constexpr int TC = NT / TR;
+    constexpr int RPT = (N + TR - 1) / TR;
+    constexpr int CPT = (NCOL + TC - 1) / TC;
+    const int tid = threadIdx.x, tr = tid % TR, tc = tid / TR, lane = tid & 31;
+    const unsigned gmask = (TR == 32) ? 0xffffffffu : (((1u << TR) - 1u) << (lane & ~(TR - 1)));
+    double a[RPT][CPT];
+#pragma unroll
+    for (int i = 0; i < RPT; i++)
+#pragma unroll
+        for (int jj = 0; jj < CPT; jj++) {
+            const int r = tr + i * TR, j = tc + jj * TC;
+            double v = 0.0;
+            if (r < N && j < NCOL) v = (j < N) ? A[r + N * j] : B[r + N * (j - N)];
+            a[i][jj] = v;
+        }
+    unsigned used = 0u;
+    // owners of column kc publish it and choose its pivot row: key = bits of (float)|v| with
+    // the low 10 bits replaced by the row (|v| within 2^-13 relative counts as a tie, won
+    // by the higher row; NaN wins so that it is reported)
+    auto publish = [&](int kc, int jq) {
+        double *pn = pcol + (kc & 1) * N;
+        unsigned best = 0u;
+#pragma unroll
+        for (int i = 0; i < RPT; i++) {
+            const int r = tr + i * TR;
+            double v = a[i][0];
+#pragma unroll
+            for (int jj = 1; jj < CPT; jj++) if (jq == jj) v = a[i][jj];
+            if (r < N) {
+                pn[r] = v;
+                if (PIVOT && !((used >> i) & 1u)) {
+                    const float av = (float)fabs(v);
+                    const unsigned key = (av == av ? (__float_as_uint(av) & ~0x3FFu) : 0xFFFFFC00u) | (unsigned)r;
+                    best = key > best ? key : best;
+                }
+            }
+        }
+        if (PIVOT) {
+#pragma unroll
+            for (int o = TR / 2; o > 0; o >>= 1) {
+                const unsigned ob = __shfl_xor_sync(gmask, best, o, TR);
+                best = ob > best ? ob : best;
+            }
+            if (tr == 0) slot[kc & 1] = (int)(best & 0x3FFu);
+        }
+    };
+    if (tc == 0) publish(0, 0);
+    __syncthreads();
+    for (int k = 0; k < N; k++) {
+        const int p = PIVOT ? slot[k & 1] : k;
+        const double *pc = pcol + (k & 1) * N;
+        const double piv = pc[p];
+        const double ipiv = (piv != 0.0) ? 1.0 / piv : 0.0;
+        if (tid == 0) {
+            diag[k] = piv;
+            rowvar[p] = k;
+            if (!(fabs(piv) > 0.0) || !isfinite(piv)) { if (*bad == 0) *bad = k + 1; }
+        }
+        if (p % TR == tr) used |= 1u << (p / TR);
+        double l[RPT];
+#pragma unroll
+        for (int i = 0; i < RPT; i++) {
+            const int r = tr + i * TR;
+            l[i] = (r < N && r != p) ? pc[r] * ipiv : 0.0;
+        }
+        const int src = (lane & ~(TR - 1)) | (p % TR);
+        const int ip = p / TR;
+#pragma unroll
+        for (int jj = 0; jj < CPT; jj++) {
+            double mine = a[0][jj];
+#pragma unroll
+            for (int i = 1; i < RPT; i++) if (ip == i) mine = a[i][jj];
+            const double pv = __shfl_sync(0xffffffffu, mine, src);
+            const int j = tc + jj * TC;
+            if (j > k) {
+#pragma unroll
+                for (int i = 0; i < RPT; i++) a[i][jj] -= l[i] * pv;
+            }
+        }
+        const int k1 = k + 1;
+        if (k1 < N && tc == k1 % TC) publish(k1, k1 / TC);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < RPT; i++)
+#pragma unroll
+        for (int jj = 0; jj < CPT; jj++) {
+            const int r = tr + i * TR, j = tc + jj * TC;
+            if (r < N && j >= N && j < NCOL) {
+                const int var = rowvar[r];
+                B[var + N * (j - N)] = a[i][jj] / diag[var];
+            }
+        }
+    __syncthreads();
+}
 }  // namespace hdgx

@@ -107,7 +107,8 @@ struct Plan {
     static constexpr int d_slots = (x_end > y_end ? x_end : y_end);   // 3 x u64 pivot slots
     static constexpr int d_pcol = d_slots + 4;                          // [4*NU] pivot column copies
     static constexpr int d_diag = d_pcol + 4 * D::NU;                   // [NU] pivots
-    static constexpr int n_doubles = d_diag + D::NU;
+    static constexpr int d_b0 = d_diag + D::NU;                         // [NU] first right-hand side
+    static constexpr int n_doubles = d_b0 + D::NU;
     // integers after the doubles
     static constexpr int i_perm = 0;                      // [NPF, NFE] 0-based
     static constexpr int i_invp = D::NPF * D::NFE;        // [NPV, NFE] face-local index or -1
@@ -331,8 +332,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
 
         // ============================ Mi = inv(M): MiC, MiE, MiRq (schur_primal.m:86-91)
         // M is SPD (exact quadrature of phi phi jac): eliminate without pivoting
-        gj_regs<NPV, NPV * ND + NDF * ND + NCU * ND, NT, 8, false>(s_M, s_MiC, s_pcol, s_diag, s_rowvar,
-                                                                  s_gslot, s_bad);
+        gj_regs_nopiv<NPV, NPV * ND + NDF * ND + NCU * ND, NT, 8>(s_M, s_MiC, s_pcol, s_bad);
         if (tid == 0 && *s_bad) *s_bad = 1;
         __syncthreads();
 
@@ -497,6 +497,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
             }
             s_SD[i] = v;
         }
+        auto build_rhs = [&]() {
         // rhs0 = Ru - B Mi Rq (volint.m:258, faceint.m:306-331; schur_primal.m:95,111)
         for (int i = tid; i < NU; i += NT) {
             const int r = i % NPV, a = i / NPV;
@@ -565,6 +566,8 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
             }
             s_R[NU + i] = v;
         }
+        };
+        build_rhs();
         // Rh = -(fbou or fhat) integrated on each face (faceint.m:335-339)
         for (int i = tid; i < NH; i += NT) {
             const int a = i % NCU, mf = i / NCU, m = mf % NPF, j = mf / NPF;
@@ -578,7 +581,63 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
         {
             int bad_before = *s_bad;
             __syncthreads();
-            gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
+            if constexpr (VISC) {
+                // the viscous local matrix needs row exchanges (the unpivoted check fails on it)
+                gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
+            } else {
+                // fast path: unpivoted elimination; accepted when the backward error of the first
+                // column, |b0 - SD x0| / (|SD| |x0| + |b0|) (infinity norms), is below 1e-13
+                double *s_b0 = sm + L::d_b0;
+                for (int i = tid; i < NU; i += NT) s_b0[i] = s_R[i];
+                __syncthreads();
+                gj_regs_nopiv<NU, 1 + NH, NT, 8>(s_SD, s_R, s_pcol, s_bad);
+                {
+                    double rmax = 0.0, amax = 0.0, xmax = 0.0, bmax = 0.0;
+                    for (int r = tid; r < NU; r += NT) {
+                        double res = s_b0[r], as = 0.0;
+                        for (int c = 0; c < NU; c++) {
+                            const double sd = s_SD[r + NU * c];
+                            res -= sd * s_R[c];
+                            as += fabs(sd);
+                        }
+                        rmax = fmax(rmax, fabs(res));
+                        amax = fmax(amax, as);
+                        xmax = fmax(xmax, fabs(s_R[r]));
+                        bmax = fmax(bmax, fabs(s_b0[r]));
+                    }
+                    if (!(rmax == rmax)) rmax = INFINITY;
+                    for (int o = 16; o > 0; o >>= 1) {
+                        rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+                        amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+                        xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+                        bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+                    }
+                    double *red = s_pcol;   // free after the elimination
+                    if ((tid & 31) == 0) {
+                        red[4 * (tid >> 5) + 0] = rmax; red[4 * (tid >> 5) + 1] = amax;
+                        red[4 * (tid >> 5) + 2] = xmax; red[4 * (tid >> 5) + 3] = bmax;
+                    }
+                    __syncthreads();
+                    if (tid == 0) {
+                        double R = 0.0, A = 0.0, X = 0.0, B = 0.0;
+                        for (int w = 0; w < NT / 32; w++) {
+                            R = fmax(R, red[4 * w]); A = fmax(A, red[4 * w + 1]);
+                            X = fmax(X, red[4 * w + 2]); B = fmax(B, red[4 * w + 3]);
+                        }
+                        const double den = A * X + B;
+                        const bool ok = (*s_bad == bad_before) && (R <= 1e-13 * den) && isfinite(R);
+                        s_gslot[0] = ok ? 0 : 1;
+                        if (!ok) *s_bad = bad_before;
+                    }
+                    __syncthreads();
+                }
+                if (s_gslot[0]) {
+                    // fall back to partial pivoting on the original system
+                    build_rhs();
+                    __syncthreads();
+                    gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
+                }
+            }
             if (tid == 0 && *s_bad && !bad_before) *s_bad = 2;
             __syncthreads();
         }

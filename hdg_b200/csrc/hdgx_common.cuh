@@ -358,4 +358,96 @@ __device__ __forceinline__ void gj_regs(const double *__restrict__ A, double *B,
         }
     __syncthreads();
 }
+// Unpivoted Gauss-Jordan on [A | B] with the matrix in registers (layout as gj_regs), the
+// step loop fully unrolled so every pivot position is a compile-time constant.  The owner
+// lane of the next pivot row publishes the next column and the reciprocal of the next
+// pivot at the end of each step.  Used for M (symmetric positive definite) and as the
+// fast path for the local matrix SD, whose result is then checked (backward error) and
+// redone with gj_regs<..., PIVOT = true> when the check fails.  *bad = k+1 for the first
+// zero or non-finite pivot.  Shared scratch: pcol[2N + 2].
+template <int N, int NR, int NT, int TR>
+__device__ __forceinline__ void gj_regs_nopiv(const double *__restrict__ A, double *B, double *pcol, int *bad) {
+    static_assert(32 % TR == 0 && NT % TR == 0, "TR must divide 32 and NT");
+    constexpr int NCOL = N + NR;
+    constexpr int TC = NT / TR;
+    constexpr int RPT = (N + TR - 1) / TR;
+    constexpr int CPT = (NCOL + TC - 1) / TC;
+    const int tid = threadIdx.x, tr = tid % TR, tc = tid / TR, lane = tid & 31;
+    double a[RPT][CPT];
+#pragma unroll
+    for (int i = 0; i < RPT; i++)
+#pragma unroll
+        for (int jj = 0; jj < CPT; jj++) {
+            const int r = tr + i * TR, j = tc + jj * TC;
+            double v = 0.0;
+            if (r < N && j < NCOL) v = (j < N) ? A[r + N * j] : B[r + N * (j - N)];
+            a[i][jj] = v;
+        }
+    // column 0 and 1/pivot_0
+    if (tc == 0) {
+#pragma unroll
+        for (int i = 0; i < RPT; i++) {
+            const int r = tr + i * TR;
+            if (r < N) pcol[r] = a[i][0];
+            if (r == 0) pcol[2 * N] = 1.0 / a[i][0];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        const double *pc = pcol + (k & 1) * N;
+        const double ipiv = pcol[2 * N + (k & 1)];
+        double l[RPT];
+#pragma unroll
+        for (int i = 0; i < RPT; i++) {
+            const int r = tr + i * TR;
+            l[i] = (r < N && r != k) ? pc[r] * ipiv : 0.0;
+        }
+        const int src = (lane & ~(TR - 1)) | (k % TR);
+#pragma unroll
+        for (int jj = 0; jj < CPT; jj++) {
+            const double pv = __shfl_sync(0xffffffffu, a[k / TR][jj], src);
+            if (tc + jj * TC > k) {
+#pragma unroll
+                for (int i = 0; i < RPT; i++) a[i][jj] -= l[i] * pv;
+            }
+        }
+        if (k + 1 < N && tc == (k + 1) % TC) {
+            double *pn = pcol + ((k + 1) & 1) * N;
+#pragma unroll
+            for (int i = 0; i < RPT; i++) {
+                const int r = tr + i * TR;
+                const double v = a[i][(k + 1) / TC];
+                if (r < N) pn[r] = v;
+                if (r == k + 1) {
+                    if (!(fabs(v) > 0.0) || !isfinite(v)) { if (*bad == 0) *bad = k + 2; }
+                    pcol[2 * N + ((k + 1) & 1)] = (v != 0.0) ? 1.0 / v : 0.0;
+                }
+            }
+        }
+        if (k == 0 && tid == 0) {
+            const double v0 = pc[0];
+            if (!(fabs(v0) > 0.0) || !isfinite(v0)) { if (*bad == 0) *bad = 1; }
+        }
+        __syncthreads();
+    }
+    // unknown k lives in row k and is divided by that row's diagonal entry (the pivot)
+#pragma unroll
+    for (int i = 0; i < RPT; i++)
+#pragma unroll
+        for (int jj = 0; jj < CPT; jj++) {
+            const int r = tr + i * TR, j = tc + jj * TC;
+            if (r < N && j == r) pcol[r] = a[i][jj];
+        }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < RPT; i++)
+#pragma unroll
+        for (int jj = 0; jj < CPT; jj++) {
+            const int r = tr + i * TR, j = tc + jj * TC;
+            if (r < N && j >= N && j < NCOL) B[r + N * (j - N)] = a[i][jj] / pcol[r];
+        }
+    __syncthreads();
+}
+
 }  // namespace hdgx

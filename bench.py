@@ -195,6 +195,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-newton", action="store_true")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--n", type=int, default=None, help="squares/cubes per side (smaller profiling cases)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.config])
@@ -225,15 +227,27 @@ def main():
     out = alloc_elemental_outputs(m, a, ne)
     stream = torch.cuda.current_stream()
 
-    def step():
+    mixed_out = alloc_elemental_outputs(m, a, ne)
+
+    def step_fp64():
         hdg_elemental(m, a, d_in["dg"], d_in["bf"], d_in["udg"], d_in["uh"], d_in["sh"], out=out,
                       stream=stream, dmaster=dm)
 
+    def step_mixed():
+        hdg_elemental(m, a, d_in["dg"], d_in["bf"], d_in["udg"], d_in["uh"], d_in["sh"], out=mixed_out,
+                      stream=stream, dmaster=dm, mixed=True)
+
     for _ in range(args.warmup):
-        step()
+        step_fp64()
+        step_mixed()
     torch.cuda.synchronize()
-    if int(out.status.numpy().max()) != 0:
+    if int(out.status.numpy().max()) != 0 or int(mixed_out.status.numpy().max()) != 0:
         raise RuntimeError("elemental kernel reported a singular element")
+    # accuracy of the mixed form on this step: condensed residual FE vs the FP64 form
+    fe_err = float((mixed_out.FE.t - out.FE.t).abs().max() / out.FE.t.abs().max())
+    ae_err = float((mixed_out.AE.t - out.AE.t).abs().max() / out.AE.t.abs().max())
+    use_mixed = args.precision == "mixed"
+    step = step_mixed if use_mixed else step_fp64
 
     sampler = ClockSampler(local)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -262,6 +276,16 @@ def main():
         total_ms = float(tt.item())
     ms_per_step = total_ms / args.steps
     value = ws * ne * args.steps / (total_ms * 1e-3)
+    # the other precision, same protocol (no clock sampling)
+    other = step_fp64 if use_mixed else step_mixed
+    o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    o0.record(stream)
+    for _ in range(args.steps):
+        other()
+    o1.record(stream)
+    torch.cuda.synchronize()
+    other_ms = o0.elapsed_time(o1) / args.steps
 
     line = None
     if rank == 0:
@@ -306,9 +330,10 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32" if use_mixed else "f64",
             "data": "synthetic (seeded PCG64 state on a generated mesh)",
-            "config": {"workload": wl["desc"], "step": "hdg_elemental over all elements (FP64, fused kernel)",
+            "config": {"workload": wl["desc"],
+                       "step": f"hdg_elemental over all elements ({'mixed-precision' if use_mixed else 'FP64'} fused kernel)",
                        "elements_per_gpu": ne, "parallelism": f"replicas x{ws} (elements independent)",
                        "l2": f"each step writes {d2h / 1e9:.2f} GB of outputs (> 126 MB L2), evicting the inputs"},
             "roofline": roof, "cpu_baseline": cpu,
@@ -317,11 +342,48 @@ def main():
             "clocks": clocks, "gpu_launches": args.steps,
             "kernel_ms": {"mean": statistics.mean(kern_ms), "min": min(kern_ms), "max": max(kern_ms)},
         }
+        fp64_ms = other_ms if use_mixed else ms_per_step
+        mixed_ms = ms_per_step if use_mixed else other_ms
+        line["precision"] = {
+            "value_is": "mixed" if use_mixed else "fp64",
+            "fp64": {"value": ne / (fp64_ms * 1e-3), "ms_per_step": fp64_ms},
+            "mixed": {"value": ne / (mixed_ms * 1e-3), "ms_per_step": mixed_ms,
+                      "FE_rel_err_vs_fp64": fe_err, "AE_rel_err_vs_fp64": ae_err,
+                      "scheme": "FP32 local elimination of the Jacobian columns, FP64-refined residual solve, FP64 residuals"},
+            "mixed_over_fp64": fp64_ms / mixed_ms,
+        }
+        if not args.no_newton and ws == 1:
+            line["newton"] = newton_step(P, torch, args)
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def newton_step(P, torch, args):
+    """One full Newton iteration (hdg_solve.m:108-176) on the device, FP64 and mixed:
+    elemental + global assembly, BILU(0) factor, GMRES to 1e-10, back-substitution, and the
+    line-search re-assembly; elements / (wall time of the iteration, synchronised)."""
+    from hdg_b200.elemental import DArray
+    from hdg_b200.solve import HDGSolver
+    res = {}
+    for tag, mixed in (("fp64", False), ("mixed", True)):
+        s = HDGSolver(P.master, P.mesh, P.app, mixed=mixed)
+        U = DArray.from_numpy(P.UDG); H = DArray.from_numpy(P.UH); S = DArray.from_numpy(P.SH)
+        s.solve(U, H, S, tol=1e-10, maxiter=1)            # warm-up (compiles nothing; first-touch)
+        U = DArray.from_numpy(P.UDG); H = DArray.from_numpy(P.UH)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rep = s.solve(U, H, S, tol=1e-10, maxiter=1)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        res[tag] = {"value": P.mesh.ne / dt, "unit": UNIT, "s": dt, "gmres_iters": rep.gmres_iters,
+                    "gmres_relres": rep.gmres_relres, "residuals": rep.residuals}
+        del s
+        torch.cuda.empty_cache()
+    res["note"] = "one Newton iteration incl. initial assembly, BILU(0)-GMRES(20) to 1e-10, back-substitution, line-search re-assembly"
+    return res
 
 
 if __name__ == "__main__":

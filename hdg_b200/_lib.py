@@ -31,7 +31,7 @@ class HdgxApp(ct.Structure):
 
 class HdgxBsr(ct.Structure):
     _fields_ = [("nf", ct.c_int), ("bs", ct.c_int), ("nnzb", ct.c_longlong), ("rowpts", _dp), ("colind", _dp),
-                ("ncolors", ct.c_int), ("color_ptr", _dp), ("color_rows", _dp), ("pos", _dp)]
+                ("ncolors", ct.c_int), ("color_ptr", _dp), ("color_rows", _dp), ("pos", _dp), ("sched", _dp)]
 
 
 class HdgxAssemblyMap(ct.Structure):
@@ -69,6 +69,8 @@ def _declare(L):
     L.hdgx_status_count.argtypes = [v, i, v]
     L.hdgx_elemental.restype = i
     L.hdgx_elemental.argtypes = [p(HdgxMaster), p(HdgxApp), i] + [v] * 10 + [v]
+    L.hdgx_elemental_mixed.restype = i
+    L.hdgx_elemental_mixed.argtypes = [p(HdgxMaster), p(HdgxApp), i] + [v] * 10 + [v]
     L.hdgx_schur_uq.restype = i
     L.hdgx_schur_uq.argtypes = [i] * 5 + [v] * 15 + [v]
     L.hdgx_schur_u.restype = i
@@ -78,6 +80,10 @@ def _declare(L):
     L.hdgx_gather_uh.argtypes = [i, i, i, v, v, v, v]
     L.hdgx_globalassembly.restype = i
     L.hdgx_globalassembly.argtypes = [B, M, i, i, i, v, v, v, v, v, v]
+    L.hdgx_block_norms.restype = i
+    L.hdgx_block_norms.argtypes = [B, v, v, v]
+    L.hdgx_mdf_ordering.restype = i
+    L.hdgx_mdf_ordering.argtypes = [i, v, v, v, v, v]
     L.hdgx_matvec.restype = i
     L.hdgx_matvec.argtypes = [B, v, v, v, v]
     L.hdgx_bilu0_factor.restype = i

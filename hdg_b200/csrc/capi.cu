@@ -6,7 +6,7 @@
 namespace hdgx {
 int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const double *dgnodes,
                      const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
-                     double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st);
+                     double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed);
 int schur_launch(int qform, int nd, int npv, int ncu, int nc, int ndf, int ne, const double *M,
                  const double *C, const double *E, const double *BD, const double *F, const double *GK,
                  const double *H, const double *Rq, const double *Ru, const double *Rh, double *DUDG,
@@ -36,6 +36,7 @@ const char *hdgx_status_str(int code) {
         case -11: return "kernel does not fit on an SM";
         case -12: return "kernel launch failed";
         case -13: return "CUDA error while counting status";
+        case -14: return "a flag-synchronised BILU(0) sweep gave up waiting (bounded spin)";
         default: return "unknown status";
     }
 }
@@ -71,7 +72,25 @@ int hdgx_elemental(const hdgx_master *master, const hdgx_app *app, int ne, const
     if (app->localsolve != 1 || app->getdqdg != 1) return -2;
     if (app->nbnd < 0 || app->nbnd > HDGX_MAX_BND) return -4;
     return hdgx::elemental_launch(master, app, ne, dgnodes, bf, UDG, UH, SH, AE, FE, DUDG, DUDG_DUH,
-                                  status, (cudaStream_t)stream);
+                                  status, (cudaStream_t)stream, false);
+}
+
+int hdgx_elemental_mixed(const hdgx_master *master, const hdgx_app *app, int ne, const double *dgnodes,
+                         const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
+                         double *FE, double *DUDG, double *DUDG_DUH, int *status, hdgx_stream_t stream) {
+    if (!master || !app || ne < 0) return -1;
+    if (ne == 0) return 0;
+    if (!dgnodes || !bf || !UDG || !UH || !SH || !AE || !FE || !DUDG || !DUDG_DUH) return -1;
+    if (!master->shapvt || !master->shapvg || !master->shapmv || !master->shapft || !master->shapfg ||
+        !master->shapmf || !master->perm)
+        return -1;
+    const int nd = master->nd;
+    if (app->nd != nd || app->ncu != nd + 2 || app->nc != (nd + 2) * (nd + 1) || master->nfe != nd + 1)
+        return -2;
+    if (app->localsolve != 1 || app->getdqdg != 1) return -2;
+    if (app->nbnd < 0 || app->nbnd > HDGX_MAX_BND) return -4;
+    return hdgx::elemental_launch(master, app, ne, dgnodes, bf, UDG, UH, SH, AE, FE, DUDG, DUDG_DUH,
+                                  status, (cudaStream_t)stream, true);
 }
 
 int hdgx_schur_uq(int nd, int npv, int ncu, int ndf, int ne, const double *M, const double *C,

@@ -1,6 +1,8 @@
 // capi_trace.cu -- extern "C" entry points of the condensed-system path (include/hdgx.h).
 #include <cuda_runtime.h>
 #include <math.h>
+#include <queue>
+#include <utility>
 #include <vector>
 #include "hdgx_common.cuh"
 
@@ -16,6 +18,14 @@ __global__ void bilu0_fwd_kernel(int, const int *, int, const long long *, const
                                  const double *, double *);
 __global__ void bilu0_bwd_kernel(int, const int *, int, const long long *, const int *, const int *, const double *,
                                  const double *, double *);
+template <int NT>
+__global__ void block_norms_kernel(int, int, const long long *, const double *, double *);
+template <int NT>
+__global__ void bilu0_sched_factor_kernel(int, int, const int *, const long long *, const int *, const int *, double *,
+                                          int *, int *);
+__global__ void bilu0_sched_sweep_kernel(int, int, int, const int *, const long long *, const int *, const int *,
+                                         const double *, const double *, double *, int *);
+__global__ void sched_begin_kernel(int *);
 __global__ void backsub_kernel(int, int, int, int, const int *, const double *, const double *, const double *, double *);
 __global__ void dot_partial_kernel(size_t, const double *, const double *, double *);
 __global__ void dot_final_kernel(int, const double *, double *, int);
@@ -53,8 +63,27 @@ static int matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *
     return launched();
 }
 
+static int resident_grid(const void *kern, int threads, size_t smem, int cap) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    int g = sm_count() * (per_sm > 0 ? per_sm : 1);
+    return g < cap ? g : cap;
+}
+
 static int bilu0_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *y, double *v, cudaStream_t st) {
     const int threads = 256, warps = threads / 32;
+    if (A->ncolors == 0) {
+        if (!A->sched) return -1;
+        const size_t smem = sizeof(double) * warps * A->bs;
+        const int grid = resident_grid((const void *)bilu0_sched_sweep_kernel, threads, smem, (A->nf + warps - 1) / warps);
+        sched_begin_kernel<<<1, 1, 0, st>>>(A->sched);
+        bilu0_sched_sweep_kernel<<<grid, threads, smem, st>>>(A->bs, A->nf, 0, A->color_rows, A->rowpts, A->colind,
+                                                              A->pos, Mg, x, y, A->sched);
+        sched_begin_kernel<<<1, 1, 0, st>>>(A->sched);
+        bilu0_sched_sweep_kernel<<<grid, threads, smem, st>>>(A->bs, A->nf, 1, A->color_rows, A->rowpts, A->colind,
+                                                              A->pos, Mg, y, v, A->sched);
+        return launched();
+    }
     for (int c = 0; c < A->ncolors; c++) {
         const int r0 = A->color_ptr[c], nr = A->color_ptr[c + 1] - r0;
         if (nr <= 0) continue;
@@ -119,6 +148,17 @@ int hdgx_bilu0_factor(const hdgx_bsr *A, double *Mg, int *status, hdgx_stream_t 
     constexpr int NT = 256;
     const size_t smem = bilu_smem(A->bs);
     if (smem > 200 * 1024) return -3;
+    if (A->ncolors == 0) {
+        if (!A->sched) return -1;
+        if (cudaFuncSetAttribute(bilu0_sched_factor_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return -10;
+        const int grid = resident_grid((const void *)bilu0_sched_factor_kernel<NT>, NT, smem, A->nf);
+        sched_begin_kernel<<<1, 1, 0, st>>>(A->sched);
+        bilu0_sched_factor_kernel<NT><<<grid, NT, smem, st>>>(A->bs, A->nf, A->color_rows, A->rowpts, A->colind, A->pos,
+                                                              Mg, A->sched, status);
+        return launched();
+    }
     if (cudaFuncSetAttribute(bilu0_color_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -10;
     for (int c = 0; c < A->ncolors; c++) {
@@ -144,6 +184,17 @@ int hdgx_backsub(int npv, int nc, int ncu, int ndf, int ne, const int *elcon, co
     unsigned g = (unsigned)(ne < sm_count() * 16 ? ne : sm_count() * 16);
     backsub_kernel<<<g, 128, sizeof(double) * nh, (cudaStream_t)stream>>>(ne, npv * nc, ncu, ndf, elcon, DUDG, DUDG_DUH,
                                                                           DUH, DUDGT);
+    return launched();
+}
+
+int hdgx_block_norms(const hdgx_bsr *A, const double *Hg, double *C, hdgx_stream_t stream) {
+    if (!A || !Hg || !C || A->bs > 128) return -1;
+    const size_t need = sizeof(double) * (2 * (size_t)A->bs * A->bs + 130 + 8);
+    if (need > 227 * 1024) return -3;
+    if (cudaFuncSetAttribute(block_norms_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) != cudaSuccess)
+        return -10;
+    const int grid = A->nf < sm_count() * 4 ? A->nf : sm_count() * 4;
+    block_norms_kernel<256><<<grid, 256, need, (cudaStream_t)stream>>>(A->bs, A->nf, A->rowpts, Hg, C);
     return launched();
 }
 
@@ -231,10 +282,65 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
     if (iters) *iters = iter;
     if (flag) *flag = fl;
     if (relres) *relres = res_rel;
+    int sched_err = 0;
+    if (A->ncolors == 0 && A->sched) {
+        cudaMemcpy(&sched_err, A->sched + 2, sizeof(int), cudaMemcpyDeviceToHost);
+        if (sched_err) cudaMemset(A->sched + 2, 0, sizeof(int));
+    }
     cudaFreeHost(h_nrmb);
     if (own) cudaFreeAsync(mem, st);
     if (cudaGetLastError() != cudaSuccess) return -12;
+    if (sched_err) return -14;
     return rc ? -12 : 0;
 }
 
 }  // extern "C"
+
+// computeMDFordering.m:21-161 with a lazy min-heap instead of the reference's linear min over
+// all rows (same choices: smallest weight, ties to the lowest row).
+extern "C" int hdgx_mdf_ordering(int nf, const long long *rowpts, const int *colind, const double *C, int *o2u,
+                                 int *u2o) {
+    if (nf < 0 || !rowpts || !colind || !C || !o2u || !u2o) return -1;
+    std::vector<char> numbered(nf, 0);
+    std::vector<double> w(nf, 0.0);
+    auto pos_in_row = [&](int row, int col1) -> long long {
+        for (long long k = rowpts[row]; k < rowpts[row + 1]; k++) if (colind[k] == col1) return k;
+        return -1;
+    };
+    auto weight = [&](int k) {
+        double acc = 0.0;
+        for (long long ni = rowpts[k] + 1; ni < rowpts[k + 1]; ni++) {
+            const int ri = colind[ni] - 1;
+            if (numbered[ri]) continue;
+            const long long ik = pos_in_row(ri, k + 1);
+            if (ik < 0) continue;
+            for (long long nj = rowpts[k] + 1; nj < rowpts[k + 1]; nj++) {
+                if (nj == ni) continue;
+                const int rj = colind[nj] - 1;
+                if (numbered[rj]) continue;
+                if (pos_in_row(ri, rj + 1) < 0) { const double d = C[ik] * C[nj]; acc += d * d; }
+            }
+        }
+        return sqrt(acc);
+    };
+    typedef std::pair<double, int> E;
+    std::priority_queue<E, std::vector<E>, std::greater<E>> heap;
+    for (int k = 0; k < nf; k++) { w[k] = weight(k); heap.push(E(w[k], k)); }
+    for (int l = 0; l < nf; l++) {
+        int p = -1;
+        while (!heap.empty()) {
+            const E e = heap.top();
+            heap.pop();
+            if (!numbered[e.second] && e.first == w[e.second]) { p = e.second; break; }
+        }
+        if (p < 0) return -2;
+        o2u[l] = p;
+        numbered[p] = 1;
+        for (long long e = rowpts[p] + 1; e < rowpts[p + 1]; e++) {
+            const int k = colind[e] - 1;
+            if (!numbered[k]) { w[k] = weight(k); heap.push(E(w[k], k)); }
+        }
+    }
+    for (int i = 0; i < nf; i++) u2o[o2u[i]] = i;
+    return 0;
+}

@@ -48,7 +48,7 @@ struct Dims {
 
 // Shared-memory plan (in doubles).  "P" = persistent through the element, "X" = the
 // assembly-phase scratch, reused by the DUDG_DUH / AE column tiles at the end.
-template <class D, bool VISC>
+template <class D, bool VISC, bool MIXED = false>
 struct Plan {
     // master tables (loaded once per CTA)
     static constexpr int t_vt = 0;
@@ -108,7 +108,8 @@ struct Plan {
     static constexpr int d_pcol = d_slots + 4;                          // [4*NU] pivot column copies
     static constexpr int d_diag = d_pcol + 4 * D::NU;                   // [NU] pivots
     static constexpr int d_b0 = d_diag + D::NU;                         // [NU] first right-hand side
-    static constexpr int n_doubles = d_b0 + D::NU;
+    static constexpr int d_inv = d_b0 + D::NU;                          // [NU*NU] FP32-accurate SD^-1 (MIXED)
+    static constexpr int n_doubles = d_inv + (MIXED ? D::NU * D::NU : 0);
     // integers after the doubles
     static constexpr int i_perm = 0;                      // [NPF, NFE] 0-based
     static constexpr int i_invp = D::NPF * D::NFE;        // [NPV, NFE] face-local index or -1
@@ -123,12 +124,17 @@ struct Plan {
     static constexpr size_t bytes = sizeof(double) * n_doubles + sizeof(int) * n_ints;
 };
 
-template <class D, bool VISC>
-constexpr int min_blocks() { return Plan<D, VISC>::bytes <= 110 * 1024 ? 2 : 1; }
+template <class D, bool VISC, bool MIXED>
+constexpr int min_blocks() { return Plan<D, VISC, MIXED>::bytes <= 110 * 1024 ? 2 : 1; }
 
-template <class D, bool VISC, int NT>
-__global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(const __grid_constant__ ElemParams P) {
-    using L = Plan<D, VISC>;
+// MIXED: the local elimination of the Jacobian columns runs in FP32 (with the identity
+// appended so that the FP32 inverse of SD comes out too); the local residual solve (DUDG)
+// is then refined against the FP64 SD to FP64 accuracy, and every residual (Ru, Rq, Rh, FE)
+// is FP64.  AE and DUDG_DUH therefore carry FP32-level errors (a Jacobian error, which
+// changes the Newton convergence rate, not the converged solution).
+template <class D, bool VISC, bool MIXED, int NT>
+__global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_kernel(const __grid_constant__ ElemParams P) {
+    using L = Plan<D, VISC, MIXED>;
     constexpr int ND = D::ND, NPV = D::NPV, NPF = D::NPF, NGV = D::NGV, NGF = D::NGF;
     constexpr int NFE = D::NFE, NCU = D::NCU, NC = D::NC, NDF = D::NDF, NU = D::NU;
     constexpr int NQ = D::NQ, NH = D::NH, NGT = D::NGT;
@@ -581,7 +587,33 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
         {
             int bad_before = *s_bad;
             __syncthreads();
-            if constexpr (VISC) {
+            if constexpr (MIXED) {
+                // FP32 elimination of [SD | R | I]; then refine the residual column in FP64
+                double *s_b0 = sm + L::d_b0;
+                double *s_inv = sm + L::d_inv;
+                for (int i = tid; i < NU; i += NT) s_b0[i] = s_R[i];
+                __syncthreads();
+                gj_regs_t<float, NU, 1 + NH, NU, true, NT, 8, true>(s_SD, s_R, s_inv, reinterpret_cast<float *>(s_pcol),
+                                                                     reinterpret_cast<float *>(s_diag), s_rowvar,
+                                                                     s_gslot, s_bad);
+                double *s_res = s_pcol;                    // free after the elimination
+                for (int it = 0; it < 3; it++) {
+                    for (int r = tid; r < NU; r += NT) {
+                        double res = s_b0[r];
+#pragma unroll 8
+                        for (int c = 0; c < NU; c++) res -= s_SD[r + NU * c] * s_R[c];
+                        s_res[r] = res;
+                    }
+                    __syncthreads();
+                    for (int r = tid; r < NU; r += NT) {
+                        double dx = 0.0;
+#pragma unroll 8
+                        for (int c = 0; c < NU; c++) dx += s_inv[r + NU * c] * s_res[c];
+                        s_R[r] += dx;
+                    }
+                    __syncthreads();
+                }
+            } else if constexpr (VISC) {
                 // the viscous local matrix needs row exchanges (the unpivoted check fails on it)
                 gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
             } else {
@@ -751,14 +783,14 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC>())) elemental_kernel(
 }
 
 // ------------------------------------------------------------------ dispatch
-template <class D, bool VISC>
+template <class D, bool VISC, bool MIXED>
 static int launch_t(const ElemParams &p, cudaStream_t st) {
     constexpr int NT = 256;
-    using L = Plan<D, VISC>;
+    using L = Plan<D, VISC, MIXED>;
     static_assert(L::TILE >= 1, "tile");
     const size_t smem = L::bytes;
     if (smem > 227 * 1024) return -3;
-    auto kern = elemental_kernel<D, VISC, NT>;
+    auto kern = elemental_kernel<D, VISC, MIXED, NT>;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return -10;
     int dev = 0, nsm = 0, per_sm = 0;
@@ -775,13 +807,14 @@ static int launch_t(const ElemParams &p, cudaStream_t st) {
 }
 
 template <class D>
-static int launch_v(const ElemParams &p, bool visc, cudaStream_t st) {
-    return visc ? launch_t<D, true>(p, st) : launch_t<D, false>(p, st);
+static int launch_v(const ElemParams &p, bool visc, bool mixed, cudaStream_t st) {
+    if (mixed) return visc ? launch_t<D, true, true>(p, st) : launch_t<D, false, true>(p, st);
+    return visc ? launch_t<D, true, false>(p, st) : launch_t<D, false, false>(p, st);
 }
 
 int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const double *dgnodes,
                      const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
-                     double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st) {
+                     double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed) {
     ElemParams p;
     p.shapvt = m->shapvt; p.shapvg = m->shapvg; p.shapmv = m->shapmv;
     p.shapft = m->shapft; p.shapfg = m->shapfg; p.shapmf = m->shapmf; p.perm = m->perm;
@@ -800,15 +833,15 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
     const int nd = m->nd, po = m->porder;
     if (nd == 2) {
         switch (po) {
-            case 1: return launch_v<Dims<2, 3, 2, 3, 2>>(p, visc, st);
-            case 2: return launch_v<Dims<2, 6, 3, 6, 3>>(p, visc, st);
-            case 3: return launch_v<Dims<2, 10, 4, 12, 4>>(p, visc, st);
-            case 4: return launch_v<Dims<2, 15, 5, 16, 5>>(p, visc, st);
+            case 1: return launch_v<Dims<2, 3, 2, 3, 2>>(p, visc, mixed, st);
+            case 2: return launch_v<Dims<2, 6, 3, 6, 3>>(p, visc, mixed, st);
+            case 3: return launch_v<Dims<2, 10, 4, 12, 4>>(p, visc, mixed, st);
+            case 4: return launch_v<Dims<2, 15, 5, 16, 5>>(p, visc, mixed, st);
         }
     } else if (nd == 3) {
         switch (po) {
-            case 1: return launch_v<Dims<3, 4, 3, 4, 3>>(p, visc, st);
-            case 2: return launch_v<Dims<3, 10, 6, 11, 6>>(p, visc, st);
+            case 1: return launch_v<Dims<3, 4, 3, 4, 3>>(p, visc, mixed, st);
+            case 2: return launch_v<Dims<3, 10, 6, 11, 6>>(p, visc, mixed, st);
         }
     }
     return -3;

@@ -258,9 +258,10 @@ __device__ void block_gauss_jordan(double *A, int lda, double *B, int ldb, int n
 // order.  PIVOT = false eliminates in natural order (SPD matrices).  *bad = k+1 for the
 // first zero or non-finite pivot.  Shared scratch: pcol[2N] (column copy, double-buffered),
 // diag[N], rowvar[N] (ints), slot[2] (ints).
-template <int N, int NR, int NT, int TR, bool PIVOT>
-__device__ __forceinline__ void gj_regs(const double *__restrict__ A, double *B, double *pcol, double *diag,
-                                        int *rowvar, int *slot, int *bad) {
+template <typename T, int N, int NR1, int NR2, bool IDENT2, int NT, int TR, bool PIVOT>
+__device__ __forceinline__ void gj_regs_t(const double *__restrict__ A, double *B, double *B2, T *pcol, T *diag,
+                                          int *rowvar, int *slot, int *bad) {
+    constexpr int NR = NR1 + NR2;
     static_assert(32 % TR == 0 && NT % TR == 0, "TR must divide 32 and NT");
     constexpr int NCOL = N + NR;
     constexpr int TC = NT / TR;
@@ -268,27 +269,31 @@ __device__ __forceinline__ void gj_regs(const double *__restrict__ A, double *B,
     constexpr int CPT = (NCOL + TC - 1) / TC;
     const int tid = threadIdx.x, tr = tid % TR, tc = tid / TR, lane = tid & 31;
     const unsigned gmask = (TR == 32) ? 0xffffffffu : (((1u << TR) - 1u) << (lane & ~(TR - 1)));
-    double a[RPT][CPT];
+    T a[RPT][CPT];
 #pragma unroll
     for (int i = 0; i < RPT; i++)
 #pragma unroll
         for (int jj = 0; jj < CPT; jj++) {
             const int r = tr + i * TR, j = tc + jj * TC;
             double v = 0.0;
-            if (r < N && j < NCOL) v = (j < N) ? A[r + N * j] : B[r + N * (j - N)];
-            a[i][jj] = v;
+            if (r < N && j < NCOL) {
+                if (j < N) v = A[r + N * j];
+                else if (j < N + NR1) v = B[r + N * (j - N)];
+                else v = IDENT2 ? ((j - N - NR1 == r) ? 1.0 : 0.0) : B2[r + N * (j - N - NR1)];
+            }
+            a[i][jj] = (T)v;
         }
     unsigned used = 0u;
     // owners of column kc publish it and choose its pivot row: key = bits of (float)|v| with
     // the low 10 bits replaced by the row (|v| within 2^-13 relative counts as a tie, won
     // by the higher row; NaN wins so that it is reported)
     auto publish = [&](int kc, int jq) {
-        double *pn = pcol + (kc & 1) * N;
+        T *pn = pcol + (kc & 1) * N;
         unsigned best = 0u;
 #pragma unroll
         for (int i = 0; i < RPT; i++) {
             const int r = tr + i * TR;
-            double v = a[i][0];
+            T v = a[i][0];
 #pragma unroll
             for (int jj = 1; jj < CPT; jj++) if (jq == jj) v = a[i][jj];
             if (r < N) {
@@ -313,29 +318,29 @@ __device__ __forceinline__ void gj_regs(const double *__restrict__ A, double *B,
     __syncthreads();
     for (int k = 0; k < N; k++) {
         const int p = PIVOT ? slot[k & 1] : k;
-        const double *pc = pcol + (k & 1) * N;
-        const double piv = pc[p];
-        const double ipiv = (piv != 0.0) ? 1.0 / piv : 0.0;
+        const T *pc = pcol + (k & 1) * N;
+        const T piv = pc[p];
+        const T ipiv = (piv != (T)0) ? (T)1 / piv : (T)0;
         if (tid == 0) {
             diag[k] = piv;
             rowvar[p] = k;
             if (!(fabs(piv) > 0.0) || !isfinite(piv)) { if (*bad == 0) *bad = k + 1; }
         }
         if (p % TR == tr) used |= 1u << (p / TR);
-        double l[RPT];
+        T l[RPT];
 #pragma unroll
         for (int i = 0; i < RPT; i++) {
             const int r = tr + i * TR;
-            l[i] = (r < N && r != p) ? pc[r] * ipiv : 0.0;
+            l[i] = (r < N && r != p) ? pc[r] * ipiv : (T)0;
         }
         const int src = (lane & ~(TR - 1)) | (p % TR);
         const int ip = p / TR;
 #pragma unroll
         for (int jj = 0; jj < CPT; jj++) {
-            double mine = a[0][jj];
+            T mine = a[0][jj];
 #pragma unroll
             for (int i = 1; i < RPT; i++) if (ip == i) mine = a[i][jj];
-            const double pv = __shfl_sync(0xffffffffu, mine, src);
+            const T pv = __shfl_sync(0xffffffffu, mine, src);
             const int j = tc + jj * TC;
             if (j > k) {
 #pragma unroll
@@ -353,11 +358,19 @@ __device__ __forceinline__ void gj_regs(const double *__restrict__ A, double *B,
             const int r = tr + i * TR, j = tc + jj * TC;
             if (r < N && j >= N && j < NCOL) {
                 const int var = rowvar[r];
-                B[var + N * (j - N)] = a[i][jj] / diag[var];
+                const double v = (double)(a[i][jj] / diag[var]);
+                if (j < N + NR1) B[var + N * (j - N)] = v;
+                else B2[var + N * (j - N - NR1)] = v;
             }
         }
     __syncthreads();
 }
+template <int N, int NR, int NT, int TR, bool PIVOT>
+__device__ __forceinline__ void gj_regs(const double *__restrict__ A, double *B, double *pcol, double *diag,
+                                        int *rowvar, int *slot, int *bad) {
+    gj_regs_t<double, N, NR, 0, false, NT, TR, PIVOT>(A, B, nullptr, pcol, diag, rowvar, slot, bad);
+}
+
 // Unpivoted Gauss-Jordan on [A | B] with the matrix in registers (layout as gj_regs), the
 // step loop fully unrolled so every pivot position is a compile-time constant.  The owner
 // lane of the next pivot row publishes the next column and the reciprocal of the next
@@ -365,23 +378,28 @@ __device__ __forceinline__ void gj_regs(const double *__restrict__ A, double *B,
 // fast path for the local matrix SD, whose result is then checked (backward error) and
 // redone with gj_regs<..., PIVOT = true> when the check fails.  *bad = k+1 for the first
 // zero or non-finite pivot.  Shared scratch: pcol[2N + 2].
-template <int N, int NR, int NT, int TR>
-__device__ __forceinline__ void gj_regs_nopiv(const double *__restrict__ A, double *B, double *pcol, int *bad) {
+template <typename T, int N, int NR1, int NR2, bool IDENT2, int NT, int TR>
+__device__ __forceinline__ void gj_regs_nopiv_t(const double *__restrict__ A, double *B, double *B2, T *pcol, int *bad) {
+    constexpr int NR = NR1 + NR2;
     static_assert(32 % TR == 0 && NT % TR == 0, "TR must divide 32 and NT");
     constexpr int NCOL = N + NR;
     constexpr int TC = NT / TR;
     constexpr int RPT = (N + TR - 1) / TR;
     constexpr int CPT = (NCOL + TC - 1) / TC;
     const int tid = threadIdx.x, tr = tid % TR, tc = tid / TR, lane = tid & 31;
-    double a[RPT][CPT];
+    T a[RPT][CPT];
 #pragma unroll
     for (int i = 0; i < RPT; i++)
 #pragma unroll
         for (int jj = 0; jj < CPT; jj++) {
             const int r = tr + i * TR, j = tc + jj * TC;
             double v = 0.0;
-            if (r < N && j < NCOL) v = (j < N) ? A[r + N * j] : B[r + N * (j - N)];
-            a[i][jj] = v;
+            if (r < N && j < NCOL) {
+                if (j < N) v = A[r + N * j];
+                else if (j < N + NR1) v = B[r + N * (j - N)];
+                else v = IDENT2 ? ((j - N - NR1 == r) ? 1.0 : 0.0) : B2[r + N * (j - N - NR1)];
+            }
+            a[i][jj] = (T)v;
         }
     // column 0 and 1/pivot_0
     if (tc == 0) {
@@ -389,44 +407,44 @@ __device__ __forceinline__ void gj_regs_nopiv(const double *__restrict__ A, doub
         for (int i = 0; i < RPT; i++) {
             const int r = tr + i * TR;
             if (r < N) pcol[r] = a[i][0];
-            if (r == 0) pcol[2 * N] = 1.0 / a[i][0];
+            if (r == 0) pcol[2 * N] = (T)1 / a[i][0];
         }
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < N; k++) {
-        const double *pc = pcol + (k & 1) * N;
-        const double ipiv = pcol[2 * N + (k & 1)];
-        double l[RPT];
+        const T *pc = pcol + (k & 1) * N;
+        const T ipiv = pcol[2 * N + (k & 1)];
+        T l[RPT];
 #pragma unroll
         for (int i = 0; i < RPT; i++) {
             const int r = tr + i * TR;
-            l[i] = (r < N && r != k) ? pc[r] * ipiv : 0.0;
+            l[i] = (r < N && r != k) ? pc[r] * ipiv : (T)0;
         }
         const int src = (lane & ~(TR - 1)) | (k % TR);
 #pragma unroll
         for (int jj = 0; jj < CPT; jj++) {
-            const double pv = __shfl_sync(0xffffffffu, a[k / TR][jj], src);
+            const T pv = __shfl_sync(0xffffffffu, a[k / TR][jj], src);
             if (tc + jj * TC > k) {
 #pragma unroll
                 for (int i = 0; i < RPT; i++) a[i][jj] -= l[i] * pv;
             }
         }
         if (k + 1 < N && tc == (k + 1) % TC) {
-            double *pn = pcol + ((k + 1) & 1) * N;
+            T *pn = pcol + ((k + 1) & 1) * N;
 #pragma unroll
             for (int i = 0; i < RPT; i++) {
                 const int r = tr + i * TR;
-                const double v = a[i][(k + 1) / TC];
+                const T v = a[i][(k + 1) / TC];
                 if (r < N) pn[r] = v;
                 if (r == k + 1) {
-                    if (!(fabs(v) > 0.0) || !isfinite(v)) { if (*bad == 0) *bad = k + 2; }
-                    pcol[2 * N + ((k + 1) & 1)] = (v != 0.0) ? 1.0 / v : 0.0;
+                    if (!(fabs((double)v) > 0.0) || !isfinite((double)v)) { if (*bad == 0) *bad = k + 2; }
+                    pcol[2 * N + ((k + 1) & 1)] = (v != (T)0) ? (T)1 / v : (T)0;
                 }
             }
         }
         if (k == 0 && tid == 0) {
-            const double v0 = pc[0];
+            const double v0 = (double)pc[0];
             if (!(fabs(v0) > 0.0) || !isfinite(v0)) { if (*bad == 0) *bad = 1; }
         }
         __syncthreads();
@@ -445,9 +463,18 @@ __device__ __forceinline__ void gj_regs_nopiv(const double *__restrict__ A, doub
 #pragma unroll
         for (int jj = 0; jj < CPT; jj++) {
             const int r = tr + i * TR, j = tc + jj * TC;
-            if (r < N && j >= N && j < NCOL) B[r + N * (j - N)] = a[i][jj] / pcol[r];
+            if (r < N && j >= N && j < NCOL) {
+                const double v = (double)(a[i][jj] / pcol[r]);
+                if (j < N + NR1) B[r + N * (j - N)] = v;
+                else B2[r + N * (j - N - NR1)] = v;
+            }
         }
     __syncthreads();
+}
+
+template <int N, int NR, int NT, int TR>
+__device__ __forceinline__ void gj_regs_nopiv(const double *__restrict__ A, double *B, double *pcol, int *bad) {
+    gj_regs_nopiv_t<double, N, NR, 0, false, NT, TR>(A, B, nullptr, pcol, bad);
 }
 
 }  // namespace hdgx

@@ -121,6 +121,7 @@ extern "C" int hdgx_gmres_bilu0_noalloc(const hdgx_bsr *A, const double *Hg, con
                                         double *x, int restart, double tol, int maxit, int *iters, int *flag,
                                         double *relres, double *history, hdgx_stream_t stream) {
     if (!A || !Hg || !Mg || !b || !x || restart < 1 || maxit < 1) return -1;
+    if (A->ncolors < 1) return -1;   // the flag-scheduled (sequential-order) sweeps are not offered here
     const size_t need = hdgx_gmres_workspace_bytes(A, restart);
     if (need == 0 || need > HDGX_NOALLOC_SCRATCH_BYTES) return -5;
     void *base = nullptr;

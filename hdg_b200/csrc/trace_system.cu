@@ -382,3 +382,209 @@ namespace hdgx {
 template __global__ void bilu0_color_kernel<256>(int, const int *, int, const long long *, const int *, const int *,
                                                  double *, int *);
 }
+
+// ===================================================================== MDF-ordered BILU(0)
+// computeMDFordering.m: C(k) = || inv(H_ii) H_ik ||_F for every block of row i.  One CTA per
+// row: Gauss-Jordan on [H_ii | H_i,row] (the row's blocks are contiguous in Hg).
+namespace hdgx {
+template <int NT>
+__global__ void __launch_bounds__(NT) block_norms_kernel(int bs, int nf, const long long *__restrict__ rowpts,
+                                                         const double *__restrict__ Hg, double *__restrict__ C) {
+    extern __shared__ __align__(16) double sm[];
+    const int b2 = bs * bs;
+    double *A = sm, *Inv = sm + b2;                       // [H_ii | I] -> inv(H_ii)
+    int *piv = reinterpret_cast<int *>(sm + 2 * b2);
+    int *rowused = piv + 128;
+    unsigned long long *slot = reinterpret_cast<unsigned long long *>(sm + 2 * b2 + 130);
+    int *bad = reinterpret_cast<int *>(slot + 4);
+    for (int i = blockIdx.x; i < nf; i += gridDim.x) {
+        const long long k0 = rowpts[i], k1 = rowpts[i + 1];
+        const double *H = Hg + (size_t)b2 * k0;
+        for (int t = threadIdx.x; t < b2; t += NT) { A[t] = H[t]; Inv[t] = ((t % bs) == (t / bs)) ? 1.0 : 0.0; }
+        if (threadIdx.x == 0) *bad = 0;
+        __syncthreads();
+        block_gauss_jordan<NT, true>(A, bs, Inv, bs, bs, bs, piv, rowused, slot, bad);
+        // row r of inv(H_ii) is in Inv row piv[r]; || inv(H_ii) H_ik ||_F, one warp per block
+        for (long long k = k0 + (threadIdx.x >> 5); k < k1; k += NT / 32) {
+            const double *B = Hg + (size_t)b2 * k;
+            double s = 0.0;
+            for (int t = threadIdx.x & 31; t < b2; t += 32) {
+                const int r = t % bs, c = t / bs;
+                double v = 0.0;
+                for (int m = 0; m < bs; m++) v += Inv[piv[r] + bs * m] * B[m + bs * c];
+                s += v * v;
+            }
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if ((threadIdx.x & 31) == 0) C[k] = sqrt(s);
+        }
+        __syncthreads();
+    }
+}
+template __global__ void block_norms_kernel<256>(int, int, const long long *, const double *, double *);
+
+// Flag-scheduled sweeps and factorisation in an arbitrary sequential order.  sched[] layout:
+// [0] epoch, [1] work counter, [2] error flag, [3] spare, [4 + i] ready flag of row i.
+// Rows are taken in order through the counter, so a row only waits for rows taken before it
+// by CTAs / warps that are already running; every wait is bounded (HDGX_SPIN_LIMIT polls),
+// after which the error flag is raised and the row proceeds.
+#define HDGX_SPIN_LIMIT (1 << 22)
+
+__device__ __forceinline__ void wait_flag(const int *flag, int epoch, int *err) {
+    int n = 0;
+    while (atomicAdd((int *)flag, 0) != epoch) {
+        if (++n > HDGX_SPIN_LIMIT) { atomicExch(err, 1); break; }
+        __nanosleep(64);
+    }
+    __threadfence();
+}
+
+__global__ void sched_begin_kernel(int *sched) {
+    sched[0] += 1;      // new epoch: every flag now reads "not ready"
+    sched[1] = 0;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) bilu0_sched_factor_kernel(int bs, int nf, const int *__restrict__ order,
+                                                                const long long *__restrict__ rowpts,
+                                                                const int *__restrict__ colind,
+                                                                const int *__restrict__ pos, double *Mg,
+                                                                int *sched, int *status) {
+    extern __shared__ __align__(16) double sm[];
+    const int b2 = bs * bs;
+    double *Aii = sm, *L = sm + b2, *T = sm + 2 * b2;
+    int *lower = reinterpret_cast<int *>(sm + 4 * b2);
+    int *nl = lower + 64;
+    int *piv = nl + 1;
+    int *rowused = piv + 128;
+    int *cur = rowused + 128;
+    unsigned long long *slot = reinterpret_cast<unsigned long long *>(sm + 4 * b2 + 200);
+    int *bad = reinterpret_cast<int *>(slot + 4);
+    const int tid = threadIdx.x;
+    const int epoch = sched[0];
+    int *flags = sched + 4, *err = sched + 2;
+    for (;;) {
+        if (tid == 0) {
+            const int q = atomicAdd(&sched[1], 1);
+            *cur = q < nf ? order[q] : -1;
+        }
+        __syncthreads();
+        const int i = *cur;
+        if (i < 0) break;
+        const long long k0 = rowpts[i], k1 = rowpts[i + 1];
+        const int pi = pos[i];
+        if (tid == 0) {
+            int n = 0;
+            for (long long k = k0 + 1; k < k1 && n < 64; k++)
+                if (pos[colind[k] - 1] < pi) lower[n++] = (int)k;
+            for (int a = 1; a < n; a++) {
+                int v = lower[a], b = a - 1;
+                while (b >= 0 && pos[colind[lower[b]] - 1] > pos[colind[v] - 1]) { lower[b + 1] = lower[b]; b--; }
+                lower[b + 1] = v;
+            }
+            *nl = n;
+            *bad = 0;
+            for (int s = 0; s < n; s++) wait_flag(flags + (colind[lower[s]] - 1), epoch, err);
+        }
+        __syncthreads();
+        for (int t = tid; t < b2; t += NT) Aii[t] = Mg[(size_t)b2 * k0 + t];
+        __syncthreads();
+        const int n = *nl;
+        for (int s = 0; s < n; s++) {
+            const long long kik = lower[s];
+            const int kr = colind[kik] - 1;
+            const long long kkk = rowpts[kr];
+            for (int t = tid; t < b2; t += NT) {
+                const int r = t % bs, c = t / bs;
+                const double *A = Mg + (size_t)b2 * kik, *D = Mg + (size_t)b2 * kkk;
+                double v = 0.0;
+                for (int m = 0; m < bs; m++) v += A[r + bs * m] * __ldcg(D + m + bs * c);
+                L[t] = v;
+            }
+            __syncthreads();
+            for (int t = tid; t < b2; t += NT) Mg[(size_t)b2 * kik + t] = L[t];
+            for (long long kk = rowpts[kr] + 1; kk < rowpts[kr + 1]; kk++) {
+                const int j = colind[kk] - 1;
+                if (pos[j] <= pos[kr]) continue;
+                long long kij = -1;
+                if (j == i) kij = k0;
+                else
+                    for (long long k = k0 + 1; k < k1; k++) if (colind[k] - 1 == j) { kij = k; break; }
+                if (kij < 0) continue;
+                const double *U = Mg + (size_t)b2 * kk;
+                double *dst = (kij == k0) ? Aii : Mg + (size_t)b2 * kij;
+                for (int t = tid; t < b2; t += NT) {
+                    const int r = t % bs, c = t / bs;
+                    double v = 0.0;
+                    for (int m = 0; m < bs; m++) v += L[r + bs * m] * __ldcg(U + m + bs * c);
+                    dst[t] -= v;
+                }
+                __syncthreads();
+            }
+            __syncthreads();
+        }
+        for (int t = tid; t < b2; t += NT) { T[t] = Aii[t]; T[b2 + t] = ((t % bs) == (t / bs)) ? 1.0 : 0.0; }
+        __syncthreads();
+        block_gauss_jordan<NT, true>(T, bs, T + b2, bs, bs, bs, piv, rowused, slot, bad);
+        for (int t = tid; t < b2; t += NT) {
+            const int r = t % bs, c = t / bs;
+            Mg[(size_t)b2 * k0 + t] = T[b2 + piv[r] + bs * c];
+        }
+        if (tid == 0 && *bad && status) status[i] = 1;
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) atomicExch(flags + i, epoch);
+    }
+}
+template __global__ void bilu0_sched_factor_kernel<256>(int, int, const int *, const long long *, const int *,
+                                                        const int *, double *, int *, int *);
+
+// Forward (dir = 0, order ascending, y = x - L y) or backward (dir = 1, order descending,
+// v = inv(U_ii)(y - U v)) sweep, one warp per row.
+__global__ void bilu0_sched_sweep_kernel(int bs, int nf, int dir, const int *__restrict__ order,
+                                         const long long *__restrict__ rowpts, const int *__restrict__ colind,
+                                         const int *__restrict__ pos, const double *__restrict__ Mg,
+                                         const double *__restrict__ in, double *out, int *sched) {
+    extern __shared__ double sh[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double *t = sh + w * bs;
+    const int epoch = sched[0];
+    int *flags = sched + 4, *err = sched + 2;
+    for (;;) {
+        int q = 0;
+        if (lane == 0) q = atomicAdd(&sched[1], 1);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= nf) break;
+        const int i = order[dir ? nf - 1 - q : q], pi = pos[i];
+        const long long k0 = rowpts[i], k1 = rowpts[i + 1];
+        if (lane == 0)
+            for (long long k = k0 + 1; k < k1; k++) {
+                const int j = colind[k] - 1;
+                if (dir ? (pos[j] > pi) : (pos[j] < pi)) wait_flag(flags + j, epoch, err);
+            }
+        __syncwarp();
+        for (int r = lane; r < bs; r += 32) {
+            double acc = in[(size_t)bs * i + r];
+            for (long long k = k0 + 1; k < k1; k++) {
+                const int j = colind[k] - 1;
+                if (dir ? (pos[j] <= pi) : (pos[j] >= pi)) continue;
+                const double *B = Mg + (size_t)bs * bs * k, *oj = out + (size_t)bs * j;
+                for (int c = 0; c < bs; c++) acc -= B[r + bs * c] * __ldcg(oj + c);
+            }
+            t[r] = acc;
+        }
+        __syncwarp();
+        for (int r = lane; r < bs; r += 32) {
+            double v = t[r];
+            if (dir) {
+                const double *D = Mg + (size_t)bs * bs * k0;
+                v = 0.0;
+                for (int c = 0; c < bs; c++) v += D[r + bs * c] * t[c];
+            }
+            out[(size_t)bs * i + r] = v;
+        }
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) atomicExch(flags + i, epoch);
+    }
+}
+}  // namespace hdgx

@@ -127,8 +127,12 @@ def alloc_elemental_outputs(master, app, ne):
                             DArray.zeros((ne,), dtype=torch.int32))
 
 
-def hdg_elemental(master, app, dgnodes, bf, UDG, UH, SH, out=None, stream=None, dmaster=None):
+def hdg_elemental(master, app, dgnodes, bf, UDG, UH, SH, out=None, stream=None, dmaster=None, mixed=False):
     """kernel/hdg_elemental.m: [AE, FE, DUDG, DUDG_DUH] for every element, on the GPU.
+
+    ``mixed=True`` selects the mixed-precision kernel (FP32 local elimination of the Jacobian
+    columns, FP64-refined residual solve): FE and DUDG stay FP64-accurate, AE and DUDG_DUH
+    carry FP32-level error.
 
     ``UH`` is the element-gathered trace ``[ncu, npf*nfe, ne]`` (hdg_assemble.m:34).
     Returns an ``ElementalOutputs`` (iterable as AE, FE, DUDG, DUDG_DUH) of ``DArray``s;
@@ -143,9 +147,10 @@ def hdg_elemental(master, app, dgnodes, bf, UDG, UH, SH, out=None, stream=None, 
     bfd = as_darray(bf, dtype=torch.int32)
     o = out if out is not None else alloc_elemental_outputs(master, app, ne)
     a = app_struct(app)
-    rc = L.hdgx_elemental(ct.byref(dm.c), ct.byref(a), ne, dg.ptr, bfd.ptr, udg.ptr, uh.ptr, sh.ptr,
-                          o.AE.ptr, o.FE.ptr, o.DUDG.ptr, o.DUDG_DUH.ptr, o.status.ptr, _stream_ptr(stream))
-    check(rc, "hdgx_elemental")
+    fn = L.hdgx_elemental_mixed if mixed else L.hdgx_elemental
+    rc = fn(ct.byref(dm.c), ct.byref(a), ne, dg.ptr, bfd.ptr, udg.ptr, uh.ptr, sh.ptr,
+            o.AE.ptr, o.FE.ptr, o.DUDG.ptr, o.DUDG_DUH.ptr, o.status.ptr, _stream_ptr(stream))
+    check(rc, "hdgx_elemental_mixed" if mixed else "hdgx_elemental")
     return o
 
 

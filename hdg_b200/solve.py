@@ -29,11 +29,21 @@ class TraceSystem:
     """Device-resident block-CSR pattern, elimination order and assembly map of a mesh."""
 
     def __init__(self, mesh, master, app, ordering=None):
+        """ordering: "mdf" (default; the reference's minimum-discarded-fill order, computed from
+        the first assembled matrix, eliminated with flag-synchronised sweeps), "multicolor"
+        (greedy colouring, one launch per colour), or an ``Ordering``."""
         _require_cuda()
         self.nf, self.npf, self.nfe, self.ncu = mesh.nf, master.npf, master.nfe, app.ncu
         self.bs = app.ncu * master.npf
         self.nnzb = int(mesh.cbsr_rowpts[-1])
-        self.ord = ordering if ordering is not None else multicolor(mesh.cbsr_rowpts, mesh.cbsr_colind, mesh.nf)
+        self.rowpts_h = np.ascontiguousarray(mesh.cbsr_rowpts, dtype=np.int64)
+        self.colind_h = np.ascontiguousarray(mesh.cbsr_colind, dtype=np.int32)
+        ordering = "mdf" if ordering is None else ordering
+        self.pending_mdf = isinstance(ordering, str) and ordering == "mdf"
+        if isinstance(ordering, str):
+            self.ord = multicolor(mesh.cbsr_rowpts, mesh.cbsr_colind, mesh.nf)
+        else:
+            self.ord = ordering
         am = assembly_map(mesh.t2f, mesh.cbsr_rowpts, mesh.cbsr_colind)
         i32 = torch.int32
         self.d = dict(
@@ -45,11 +55,39 @@ class TraceSystem:
             blk_row=DArray.from_numpy(am.blk_row, dtype=i32), face_e=DArray.from_numpy(am.face_e, dtype=i32),
             face_a=DArray.from_numpy(am.face_a, dtype=i32), elcon=DArray.from_numpy(mesh.elcon, dtype=i32))
         self.color_ptr = np.ascontiguousarray(self.ord.color_ptr, dtype=np.int32)
+        self.sched = torch.zeros(4 + self.nf, dtype=torch.int32, device="cuda")
         d = self.d
         self.bsr = HdgxBsr(self.nf, self.bs, self.nnzb, d["rowpts"].ptr, d["colind"].ptr, self.ord.ncolors,
-                           self.color_ptr.ctypes.data, d["color_rows"].ptr, d["pos"].ptr)
+                           self.color_ptr.ctypes.data, d["color_rows"].ptr, d["pos"].ptr, None)
         self.map = HdgxAssemblyMap(d["blk_e"].ptr, d["blk_ab"].ptr, d["blk_row"].ptr, d["face_e"].ptr,
                                    d["face_a"].ptr)
+
+    def set_order(self, o2u, u2o):
+        """Eliminate rows one after another in the order o2u (flag-synchronised sweeps)."""
+        self.o2u = np.ascontiguousarray(o2u, dtype=np.int32)
+        self.u2o = np.ascontiguousarray(u2o, dtype=np.int32)
+        self.d["color_rows"] = DArray.from_numpy(self.o2u, dtype=torch.int32)
+        self.d["pos"] = DArray.from_numpy(self.u2o, dtype=torch.int32)
+        self.color_ptr = np.array([0, self.nf], dtype=np.int32)
+        self.sched.zero_()
+        self.bsr.ncolors = 0
+        self.bsr.color_ptr = self.color_ptr.ctypes.data
+        self.bsr.color_rows = self.d["color_rows"].ptr
+        self.bsr.pos = self.d["pos"].ptr
+        self.bsr.sched = self.sched.data_ptr()
+        self.pending_mdf = False
+
+    def mdf_order(self, Hg, stream=None):
+        """computeMDFordering.m: block norms on the GPU, greedy selection on the host."""
+        C = torch.empty(self.nnzb, dtype=torch.float64, device="cuda")
+        check(lib().hdgx_block_norms(ct.byref(self.bsr), Hg.ptr, C.data_ptr(), _stream_ptr(stream)), "hdgx_block_norms")
+        Ch = np.ascontiguousarray(C.cpu().numpy())
+        o2u = np.zeros(self.nf, dtype=np.int32)
+        u2o = np.zeros(self.nf, dtype=np.int32)
+        rc = lib().hdgx_mdf_ordering(self.nf, self.rowpts_h.ctypes.data, self.colind_h.ctypes.data, Ch.ctypes.data,
+                                     o2u.ctypes.data, u2o.ctypes.data)
+        check(rc, "hdgx_mdf_ordering")
+        return o2u, u2o
 
     def empty_blocks(self):
         return DArray.empty((self.bs, self.bs, self.nnzb))
@@ -67,6 +105,8 @@ class TraceSystem:
         check(lib().hdgx_matvec(ct.byref(self.bsr), Hg.ptr, x.ptr, y.ptr, _stream_ptr(stream)), "hdgx_matvec")
 
     def bilu0(self, Hg, Mg, status=None, stream=None):
+        if self.pending_mdf:
+            self.set_order(*self.mdf_order(Hg, stream))
         Mg.t.copy_(Hg.t)
         st = status.ptr if status is not None else None
         check(lib().hdgx_bilu0_factor(ct.byref(self.bsr), Mg.ptr, st, _stream_ptr(stream)), "hdgx_bilu0_factor")
@@ -104,9 +144,10 @@ class SolveReport:
 class HDGSolver:
     """Device-resident state of one steady problem (mesh, master, app) for Newton steps."""
 
-    def __init__(self, master, mesh, app, ordering=None, restart=20):
+    def __init__(self, master, mesh, app, ordering=None, restart=20, mixed=False):
         _require_cuda()
         self.master, self.mesh, self.app = master, mesh, app
+        self.mixed = mixed
         self.dm = DeviceMaster(master)
         self.ts = TraceSystem(mesh, master, app, ordering)
         ne = mesh.ne
@@ -136,9 +177,10 @@ class HDGSolver:
         self.gather(UH, stream)
         L = lib()
         o = self.out
-        rc = L.hdgx_elemental(ct.byref(self.dm.c), ct.byref(self.app_c), self.ne, self.dg.ptr, self.bf.ptr, UDG.ptr,
-                              self.UHe.ptr, SH.ptr, o.AE.ptr, o.FE.ptr, o.DUDG.ptr, o.DUDG_DUH.ptr, o.status.ptr,
-                              _stream_ptr(stream))
+        fn = L.hdgx_elemental_mixed if self.mixed else L.hdgx_elemental
+        rc = fn(ct.byref(self.dm.c), ct.byref(self.app_c), self.ne, self.dg.ptr, self.bf.ptr, UDG.ptr,
+                self.UHe.ptr, SH.ptr, o.AE.ptr, o.FE.ptr, o.DUDG.ptr, o.DUDG_DUH.ptr, o.status.ptr,
+                _stream_ptr(stream))
         check(rc, "hdgx_elemental")
         self.ts.assemble(o.AE, o.FE, self.Hg, self.Rg, stream)
         return float(torch.linalg.vector_norm(self.Rg.t).item())
@@ -203,9 +245,10 @@ class HDGSolver:
 
 
 def hdg_solve(master, mesh, app, UDG, UH, SH=None, tol=1e-10, maxiter=16, gmres_tol=1e-10, restart=20,
-              ordering=None):
-    """kernel/hdg_solve.m: returns (UDG, UH, report) as host arrays (inputs are not modified)."""
-    s = HDGSolver(master, mesh, app, ordering=ordering, restart=restart)
+              ordering=None, mixed=False):
+    """kernel/hdg_solve.m: returns (UDG, UH, report) as host arrays (inputs are not modified).
+    ``mixed=True`` assembles with the mixed-precision elemental kernel."""
+    s = HDGSolver(master, mesh, app, ordering=ordering, restart=restart, mixed=mixed)
     dU = DArray.from_numpy(UDG)
     dH = DArray.from_numpy(UH)
     dS = DArray.from_numpy(np.zeros_like(UDG) if SH is None else SH)

@@ -80,6 +80,16 @@ int hdgx_elemental(const hdgx_master *master, const hdgx_app *app, int ne,
                    const double *SH, double *AE, double *FE, double *DUDG, double *DUDG_DUH,
                    int *status, hdgx_stream_t stream);
 
+/* Mixed-precision form of hdgx_elemental (same arguments and layouts; replaces the same
+ * kernel/hdg_elemental.m call).  The local elimination of the Jacobian columns runs in FP32
+ * and the local residual solve is refined against the FP64 local matrix, so FE and DUDG
+ * are FP64-accurate residual quantities while AE and DUDG_DUH carry FP32-level error (a
+ * Jacobian error: Newton converges to the same FP64 solution).  status 4: refinement failed. */
+int hdgx_elemental_mixed(const hdgx_master *master, const hdgx_app *app, int ne,
+                         const double *dgnodes, const int *bf, const double *UDG, const double *UH,
+                         const double *SH, double *AE, double *FE, double *DUDG, double *DUDG_DUH,
+                         int *status, hdgx_stream_t stream);
+
 /* Batched local (u,q) Schur complement on the reference MEX layouts (kernel/schur_uq.c):
  * M[npv,npv,ne] C[npv,npv,nd,ne] E[npv,ndf,nd,ne] BD[npv,ncu,npv,nc,ne] F[npv,ncu,ncu,ndf,ne]
  * GK[ncu,ndf,npv,nc,ne] H[ncu,ndf,ncu,ndf,ne] Rq[npv,ncu,nd,ne] Ru[npv,ncu,ne] Rh[ncu,ndf,ne]
@@ -114,6 +124,10 @@ typedef struct {
     const int *color_ptr;      /* HOST [ncolors+1] offsets into color_rows */
     const int *color_rows;     /* [nf] 0-based rows grouped by colour */
     const int *pos;            /* [nf] elimination position of each row */
+    int *sched;                /* ncolors == 0 only: device workspace of 4 + nf ints, zeroed once by
+                                  the caller.  Rows are then eliminated one after another in the
+                                  order color_rows (e.g. the MDF order of computeMDFordering.m), with
+                                  flag-synchronised (not level-synchronised) parallel sweeps. */
 } hdgx_bsr;
 
 /* Element -> block gather map for hdgx_globalassembly (device pointers):
@@ -134,6 +148,14 @@ int hdgx_gather_uh(int ncu, int ndf, int ne, const int *elcon, const double *UH,
 int hdgx_globalassembly(const hdgx_bsr *A, const hdgx_assembly_map *map, int ncu, int npf, int nfe,
                         const int *elcon, const double *AE, const double *FE, double *Hg, double *Rg,
                         hdgx_stream_t stream);
+
+/* C[k] = || inv(H_ii) H_ik ||_F for every block k of row i (kernel/computeMDFordering.m:14-20). */
+int hdgx_block_norms(const hdgx_bsr *A, const double *Hg, double *C, hdgx_stream_t stream);
+
+/* Minimum-discarded-fill order (kernel/computeMDFordering.m:21-161) from the block norms C
+ * (HOST arrays rowpts[nf+1], colind[nnzb], C[nnzb]); o2u[l] = row pivoted at step l, u2o its
+ * inverse (0-based, HOST).  Ties go to the lowest row, as MATLAB's min does. */
+int hdgx_mdf_ordering(int nf, const long long *rowpts, const int *colind, const double *C, int *o2u, int *u2o);
 
 /* y = Hg x (kernel/matvec.m). */
 int hdgx_matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *y, hdgx_stream_t stream);

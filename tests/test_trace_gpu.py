@@ -16,14 +16,33 @@ def rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-def _setup(oracle, name, kw):
+def _setup(oracle, name, kw, ordering="multicolor"):
     from hdg_b200.elemental import DArray
     from hdg_b200.solve import TraceSystem
     P = configs.by_name(name, **kw)
     r = oracle.hdg_elemental(P.master, P.app, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), P.SH)
     Hg, Rg = oracle.globalassembly(P.mesh, r["AE"], r["FE"], P.master.npf, P.app.ncu)
-    ts = TraceSystem(P.mesh, P.master, P.app)
+    ts = TraceSystem(P.mesh, P.master, P.app, ordering=ordering)
+    if ordering == "mdf":
+        o2u, u2o = ts.mdf_order(DArray.from_numpy(Hg))
+        ts.set_order(o2u, u2o)
     return P, r, Hg, Rg, ts, DArray
+
+
+def _order(ts):
+    if ts.bsr.ncolors == 0:
+        return ts.o2u, ts.u2o
+    return ts.ord.o2u, ts.ord.u2o
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw", CASES)
+def test_mdf_order_matches_oracle(oracle, name, kw):
+    """The product's MDF order (GPU block norms + host heap) equals the oracle's restatement
+    of computeMDFordering.m."""
+    P, r, Hg, Rg, ts, DArray = _setup(oracle, name, kw, "mdf")
+    o2u_ref, _ = oracle.mdf_ordering(P.mesh, Hg)
+    assert np.array_equal(ts.o2u, o2u_ref)
 
 
 @pytest.mark.gpu
@@ -41,11 +60,12 @@ def test_globalassembly_matvec(oracle, name, kw):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("ordering", ["multicolor", "mdf"])
 @pytest.mark.parametrize("name,kw", CASES)
-def test_bilu0_factor_and_apply_same_order(oracle, name, kw):
-    P, r, Hg, Rg, ts, DArray = _setup(oracle, name, kw)
-    o = ts.ord
-    Mg_ref, rc = oracle.bilu0(P.mesh, Hg, o.o2u, o.u2o)
+def test_bilu0_factor_and_apply_same_order(oracle, name, kw, ordering):
+    P, r, Hg, Rg, ts, DArray = _setup(oracle, name, kw, ordering)
+    o2u, u2o = _order(ts)
+    Mg_ref, rc = oracle.bilu0(P.mesh, Hg, o2u, u2o)
     assert rc == 0
     dH, dM = DArray.from_numpy(Hg), ts.empty_blocks()
     ts.bilu0(dH, dM)
@@ -53,16 +73,17 @@ def test_bilu0_factor_and_apply_same_order(oracle, name, kw):
     x = np.random.default_rng(1).standard_normal(Rg.shape)
     v, w = ts.empty_vec(), ts.empty_vec()
     ts.bilu0_apply(dM, DArray.from_numpy(x), v, w)
-    assert rel(v.numpy(), oracle.bilu0_apply(P.mesh, Mg_ref, x, o.o2u, o.u2o)) < 1e-12
+    assert rel(v.numpy(), oracle.bilu0_apply(P.mesh, Mg_ref, x, o2u, u2o)) < 1e-12
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("ordering", ["multicolor", "mdf"])
 @pytest.mark.parametrize("name,kw", CASES)
-def test_gmres_solution(oracle, name, kw):
-    P, r, Hg, Rg, ts, DArray = _setup(oracle, name, kw)
-    o = ts.ord
-    Mg_ref, _ = oracle.bilu0(P.mesh, Hg, o.o2u, o.u2o)
-    x_ref, flag, it_ref, _ = oracle.gmres_bilu0(P.mesh, Mg_ref, Hg, Rg, np.zeros_like(Rg), o.o2u, o.u2o, 20, 1e-10, 1000)
+def test_gmres_solution(oracle, name, kw, ordering):
+    P, r, Hg, Rg, ts, DArray = _setup(oracle, name, kw, ordering)
+    o2u, u2o = _order(ts)
+    Mg_ref, _ = oracle.bilu0(P.mesh, Hg, o2u, u2o)
+    x_ref, flag, it_ref, _ = oracle.gmres_bilu0(P.mesh, Mg_ref, Hg, Rg, np.zeros_like(Rg), o2u, u2o, 20, 1e-10, 1000)
     assert flag == 0
     dH, dM, dR, dx = DArray.from_numpy(Hg), ts.empty_blocks(), DArray.from_numpy(Rg), ts.empty_vec()
     ts.bilu0(dH, dM)
@@ -107,4 +128,21 @@ def test_newton_matches_oracle(oracle, name, kw):
     assert len(rep.residuals) == len(res_ref)
     for a, b in zip(rep.residuals[:-1], res_ref[:-1]):
         assert abs(a - b) <= 1e-6 * max(b, 1e-300) + 1e-12 * res_ref[0]
+    assert rel(U, U_ref) < 1e-8 and rel(H, H_ref) < 1e-8
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw", [("c1", dict(n=8)), ("c2", dict(n=6)), ("c4", dict(n=2))])
+def test_newton_mdf_matches_oracle(oracle, name, kw):
+    """Default (MDF-ordered) GPU Newton against the oracle's MDF-ordered Newton."""
+    from hdg_b200.solve import hdg_solve
+    P = configs.by_name(name, **kw)
+    U_ref, H_ref, res_ref, g_ref, a_ref = oracle.hdg_solve(P, tol=1e-10, maxiter=12)
+    U, H, rep = hdg_solve(P.master, P.mesh, P.app, P.UDG, P.UH, P.SH, tol=1e-10, maxiter=12)
+    assert rep.converged
+    assert len(rep.residuals) == len(res_ref)
+    for a, b in zip(rep.residuals[:-1], res_ref[:-1]):
+        assert abs(a - b) <= 1e-6 * max(b, 1e-300) + 1e-12 * res_ref[0]
+    for gi, gr in zip(rep.gmres_iters, g_ref):
+        assert abs(gi - gr) <= 2
     assert rel(U, U_ref) < 1e-8 and rel(H, H_ref) < 1e-8

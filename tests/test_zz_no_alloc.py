@@ -22,7 +22,7 @@ def _system(oracle):
     P = configs.c1(n=6, porder=2)
     r = oracle.hdg_elemental(P.master, P.app, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), P.SH)
     Hg, Rg = oracle.globalassembly(P.mesh, r["AE"], r["FE"], P.master.npf, P.app.ncu)
-    ts = TraceSystem(P.mesh, P.master, P.app)
+    ts = TraceSystem(P.mesh, P.master, P.app, ordering="multicolor")
     dH, dM, dR = DArray.from_numpy(Hg), ts.empty_blocks(), DArray.from_numpy(Rg)
     ts.bilu0(dH, dM)
     return ts, dH, dM, dR, Rg

@@ -41,6 +41,15 @@ __global__ void givens_kernel(GmresState, int, int);
 __global__ void hess_solve_kernel(GmresState, int, int);
 __global__ void gmres_init_kernel(GmresState, int);
 
+template <int BS>
+__global__ void bilu0_fwd_bs_kernel(const int *, int, const long long *, const int *, const int *, const double *,
+                                    const double *, double *);
+template <int BS>
+__global__ void bilu0_bwd_bs_kernel(const int *, int, const long long *, const int *, const int *, const double *,
+                                    const double *, double *);
+template <int BS>
+__global__ void bsr_matvec_bs_kernel(int, const long long *, const int *, const double *, const double *, double *);
+
 static int sm_count() {
     static int n = 0;
     if (!n) { int d = 0; cudaGetDevice(&d); cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d); }
@@ -59,8 +68,33 @@ static size_t bilu_smem(int bs) { return sizeof(double) * (4 * (size_t)bs * bs +
 static int matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *y, cudaStream_t st) {
     const int threads = 256;
     const unsigned grid = grid_for((size_t)A->nf * 32, threads);
-    bsr_matvec_kernel<<<grid, threads, 0, st>>>(A->nf, A->bs, A->rowpts, A->colind, Hg, x, y);
+    switch (A->bs) {
+#define HDGX_MV(B) case B: bsr_matvec_bs_kernel<B><<<grid, threads, 0, st>>>(A->nf, A->rowpts, A->colind, Hg, x, y); break;
+        HDGX_MV(8) HDGX_MV(12) HDGX_MV(15) HDGX_MV(16) HDGX_MV(20) HDGX_MV(30)
+#undef HDGX_MV
+        default: bsr_matvec_kernel<<<grid, threads, 0, st>>>(A->nf, A->bs, A->rowpts, A->colind, Hg, x, y);
+    }
     return launched();
+}
+
+// one colour (or level) of the forward / backward sweep, block-size specialised when possible
+static void sweep_color(const hdgx_bsr *A, int dir, const int *rows, int nr, const double *Mg, const double *in,
+                        double *out, cudaStream_t st) {
+    const int threads = 256, warps = threads / 32;
+    const unsigned grid = (unsigned)((nr + warps - 1) / warps);
+    switch (A->bs) {
+#define HDGX_SW(B)                                                                                                   \
+    case B:                                                                                                           \
+        if (dir == 0) bilu0_fwd_bs_kernel<B><<<grid, threads, 0, st>>>(rows, nr, A->rowpts, A->colind, A->pos, Mg, in, out); \
+        else bilu0_bwd_bs_kernel<B><<<grid, threads, 0, st>>>(rows, nr, A->rowpts, A->colind, A->pos, Mg, in, out);          \
+        return;
+        HDGX_SW(8) HDGX_SW(12) HDGX_SW(15) HDGX_SW(16) HDGX_SW(20) HDGX_SW(30)
+#undef HDGX_SW
+        default: break;
+    }
+    if (dir == 0) bilu0_fwd_kernel<<<grid, threads, 0, st>>>(A->bs, rows, nr, A->rowpts, A->colind, A->pos, Mg, in, out);
+    else bilu0_bwd_kernel<<<grid, threads, sizeof(double) * warps * A->bs, st>>>(A->bs, rows, nr, A->rowpts, A->colind,
+                                                                                  A->pos, Mg, in, out);
 }
 
 static int resident_grid(const void *kern, int threads, size_t smem, int cap) {
@@ -84,18 +118,14 @@ static int bilu0_apply(const hdgx_bsr *A, const double *Mg, const double *x, dou
                                                               A->pos, Mg, y, v, A->sched);
         return launched();
     }
+    (void)warps;
     for (int c = 0; c < A->ncolors; c++) {
         const int r0 = A->color_ptr[c], nr = A->color_ptr[c + 1] - r0;
-        if (nr <= 0) continue;
-        unsigned grid = (unsigned)((nr + warps - 1) / warps);
-        bilu0_fwd_kernel<<<grid, threads, 0, st>>>(A->bs, A->color_rows + r0, nr, A->rowpts, A->colind, A->pos, Mg, x, y);
+        if (nr > 0) sweep_color(A, 0, A->color_rows + r0, nr, Mg, x, y, st);
     }
     for (int c = A->ncolors - 1; c >= 0; c--) {
         const int r0 = A->color_ptr[c], nr = A->color_ptr[c + 1] - r0;
-        if (nr <= 0) continue;
-        unsigned grid = (unsigned)((nr + warps - 1) / warps);
-        bilu0_bwd_kernel<<<grid, threads, sizeof(double) * warps * A->bs, st>>>(A->bs, A->color_rows + r0, nr, A->rowpts,
-                                                                                  A->colind, A->pos, Mg, y, v);
+        if (nr > 0) sweep_color(A, 1, A->color_rows + r0, nr, Mg, y, v, st);
     }
     return launched();
 }

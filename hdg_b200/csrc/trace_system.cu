@@ -429,13 +429,18 @@ template __global__ void block_norms_kernel<256>(int, int, const long long *, co
 // after which the error flag is raised and the row proceeds.
 #define HDGX_SPIN_LIMIT (1 << 22)
 
+__device__ __forceinline__ int load_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ void wait_flag(const int *flag, int epoch, int *err) {
     int n = 0;
-    while (atomicAdd((int *)flag, 0) != epoch) {
+    while (load_acquire(flag) != epoch) {
         if (++n > HDGX_SPIN_LIMIT) { atomicExch(err, 1); break; }
-        __nanosleep(64);
+        if (n > 64) __nanosleep(64);
     }
-    __threadfence();
 }
 
 __global__ void sched_begin_kernel(int *sched) {
@@ -582,9 +587,109 @@ __global__ void bilu0_sched_sweep_kernel(int bs, int nf, int dir, const int *__r
             }
             out[(size_t)bs * i + r] = v;
         }
-        __threadfence();
         __syncwarp();
-        if (lane == 0) atomicExch(flags + i, epoch);
+        if (lane == 0) {
+            __threadfence();
+            atomicExch(flags + i, epoch);
+        }
     }
 }
+}  // namespace hdgx
+
+// ------------------------------------------------------------------------------------------
+// Block-size-specialised sweeps and matvec (BS known at compile time: every load of a block
+// row is issued before the first multiply-add, so one memory latency covers a whole block).
+namespace hdgx {
+template <int BS>
+__global__ void bilu0_fwd_bs_kernel(const int *__restrict__ rows, int nrows, const long long *__restrict__ rowpts,
+                                    const int *__restrict__ colind, const int *__restrict__ pos,
+                                    const double *__restrict__ Mg, const double *__restrict__ x, double *y) {
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    for (int q = blockIdx.x * warps + (threadIdx.x >> 5); q < nrows; q += gridDim.x * warps) {
+        const int i = rows[q], pi = pos[i];
+        for (int r = lane; r < BS; r += 32) {
+            double acc = x[(size_t)BS * i + r];
+            for (long long k = rowpts[i] + 1; k < rowpts[i + 1]; k++) {
+                const int j = colind[k] - 1;
+                if (pos[j] >= pi) continue;
+                const double *Lk = Mg + (size_t)BS * BS * k, *yj = y + (size_t)BS * j;
+                double lv[BS], yv[BS];
+#pragma unroll
+                for (int c = 0; c < BS; c++) { lv[c] = Lk[r + BS * c]; yv[c] = __ldcg(yj + c); }
+#pragma unroll
+                for (int c = 0; c < BS; c++) acc -= lv[c] * yv[c];
+            }
+            y[(size_t)BS * i + r] = acc;
+        }
+    }
+}
+
+template <int BS>
+__global__ void bilu0_bwd_bs_kernel(const int *__restrict__ rows, int nrows, const long long *__restrict__ rowpts,
+                                    const int *__restrict__ colind, const int *__restrict__ pos,
+                                    const double *__restrict__ Mg, const double *__restrict__ y, double *v) {
+    __shared__ double tsh[8][BS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    for (int q = blockIdx.x * warps + w; q < nrows; q += gridDim.x * warps) {
+        const int i = rows[q], pi = pos[i];
+        for (int r = lane; r < BS; r += 32) {
+            double acc = y[(size_t)BS * i + r];
+            for (long long k = rowpts[i] + 1; k < rowpts[i + 1]; k++) {
+                const int j = colind[k] - 1;
+                if (pos[j] <= pi) continue;
+                const double *U = Mg + (size_t)BS * BS * k, *vj = v + (size_t)BS * j;
+                double uv[BS], vv[BS];
+#pragma unroll
+                for (int c = 0; c < BS; c++) { uv[c] = U[r + BS * c]; vv[c] = __ldcg(vj + c); }
+#pragma unroll
+                for (int c = 0; c < BS; c++) acc -= uv[c] * vv[c];
+            }
+            tsh[w][r] = acc;
+        }
+        __syncwarp();
+        const double *D = Mg + (size_t)BS * BS * rowpts[i];
+        for (int r = lane; r < BS; r += 32) {
+            double dv[BS];
+#pragma unroll
+            for (int c = 0; c < BS; c++) dv[c] = D[r + BS * c];
+            double s = 0.0;
+#pragma unroll
+            for (int c = 0; c < BS; c++) s += dv[c] * tsh[w][c];
+            v[(size_t)BS * i + r] = s;
+        }
+        __syncwarp();
+    }
+}
+
+template <int BS>
+__global__ void bsr_matvec_bs_kernel(int nf, const long long *__restrict__ rowpts, const int *__restrict__ colind,
+                                     const double *__restrict__ Hg, const double *__restrict__ x,
+                                     double *__restrict__ y) {
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    for (int i = blockIdx.x * warps + (threadIdx.x >> 5); i < nf; i += gridDim.x * warps) {
+        for (int r = lane; r < BS; r += 32) {
+            double acc = 0.0;
+            for (long long k = rowpts[i]; k < rowpts[i + 1]; k++) {
+                const double *H = Hg + (size_t)BS * BS * k, *xj = x + (size_t)BS * (colind[k] - 1);
+                double hv[BS], xv[BS];
+#pragma unroll
+                for (int c = 0; c < BS; c++) { hv[c] = H[r + BS * c]; xv[c] = xj[c]; }
+#pragma unroll
+                for (int c = 0; c < BS; c++) acc += hv[c] * xv[c];
+            }
+            y[(size_t)BS * i + r] = acc;
+        }
+    }
+}
+
+#define HDGX_BS_LIST(X) X(8) X(12) X(15) X(16) X(20) X(30)
+#define HDGX_INST(B)                                                                                             \
+    template __global__ void bilu0_fwd_bs_kernel<B>(const int *, int, const long long *, const int *, const int *, \
+                                                    const double *, const double *, double *);                     \
+    template __global__ void bilu0_bwd_bs_kernel<B>(const int *, int, const long long *, const int *, const int *, \
+                                                    const double *, const double *, double *);                     \
+    template __global__ void bsr_matvec_bs_kernel<B>(int, const long long *, const int *, const double *,           \
+                                                     const double *, double *);
+HDGX_BS_LIST(HDGX_INST)
+#undef HDGX_INST
 }  // namespace hdgx

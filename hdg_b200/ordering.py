@@ -97,3 +97,27 @@ def assembly_map(t2f, rowpts, colind):
                 fill[k] += 1
     assert fill.max() <= 2 and ffill.max() <= 2
     return AssemblyMap(blk_e.ravel(), blk_ab.ravel(), blk_row, face_e.ravel(), face_a.ravel())
+
+
+def levels_of_order(rowpts, colind, o2u, u2o):
+    """Level schedule of a sequential elimination order: level(i) = 1 + max level of the
+    neighbours eliminated before i.  ILU(0) factors depend only on which of two coupled
+    rows comes first, so eliminating level by level (rows of a level share no block) gives
+    exactly the factors of the sequential order.  Returns an Ordering whose "colours" are
+    the levels and whose positions are the sequential order's."""
+    nf = len(o2u)
+    lev = np.zeros(nf, dtype=np.int64)
+    rp = np.asarray(rowpts)
+    ci = np.asarray(colind) - 1
+    u2o = np.asarray(u2o)
+    for j in range(nf):
+        i = int(o2u[j])
+        nb = ci[rp[i] + 1:rp[i + 1]]
+        low = nb[u2o[nb] < j]
+        lev[i] = lev[low].max() + 1 if low.size else 0
+    nlev = int(lev.max()) + 1
+    rows = np.lexsort((u2o, lev)).astype(np.int32)       # by level, then by position
+    counts = np.bincount(lev, minlength=nlev)
+    ptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+    return Ordering(nlev, ptr, rows, np.asarray(u2o, dtype=np.int32), np.asarray(o2u, dtype=np.int32),
+                    np.asarray(u2o, dtype=np.int32))

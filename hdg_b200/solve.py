@@ -22,7 +22,7 @@ import torch
 from ._lib import HdgxAssemblyMap, HdgxBsr, check, lib
 from .elemental import (DArray, DeviceMaster, alloc_elemental_outputs, app_struct, as_darray, _require_cuda,
                         _stream_ptr)
-from .ordering import assembly_map, multicolor
+from .ordering import assembly_map, levels_of_order, multicolor
 
 
 class TraceSystem:
@@ -57,10 +57,28 @@ class TraceSystem:
         self.color_ptr = np.ascontiguousarray(self.ord.color_ptr, dtype=np.int32)
         self.sched = torch.zeros(4 + self.nf, dtype=torch.int32, device="cuda")
         d = self.d
+        d["color_ptr"] = DArray.from_numpy(self.color_ptr, dtype=torch.int32)
         self.bsr = HdgxBsr(self.nf, self.bs, self.nnzb, d["rowpts"].ptr, d["colind"].ptr, self.ord.ncolors,
                            self.color_ptr.ctypes.data, d["color_rows"].ptr, d["pos"].ptr, None)
         self.map = HdgxAssemblyMap(d["blk_e"].ptr, d["blk_ab"].ptr, d["blk_row"].ptr, d["face_e"].ptr,
                                    d["face_a"].ptr)
+
+    def set_levels(self, o2u, u2o):
+        """Eliminate in the sequential order o2u, level by level (one launch per level)."""
+        self.o2u = np.ascontiguousarray(o2u, dtype=np.int32)
+        self.u2o = np.ascontiguousarray(u2o, dtype=np.int32)
+        lv = levels_of_order(self.rowpts_h, self.colind_h, self.o2u, self.u2o)
+        self.ord = lv
+        self.d["color_rows"] = DArray.from_numpy(lv.color_rows, dtype=torch.int32)
+        self.d["pos"] = DArray.from_numpy(lv.pos, dtype=torch.int32)
+        self.color_ptr = np.ascontiguousarray(lv.color_ptr, dtype=np.int32)
+        self.d["color_ptr"] = DArray.from_numpy(self.color_ptr, dtype=torch.int32)
+        self.bsr.ncolors = lv.ncolors
+        self.bsr.color_ptr = self.color_ptr.ctypes.data
+        self.bsr.color_rows = self.d["color_rows"].ptr
+        self.bsr.pos = self.d["pos"].ptr
+        self.bsr.sched = None
+        self.pending_mdf = False
 
     def set_order(self, o2u, u2o):
         """Eliminate rows one after another in the order o2u (flag-synchronised sweeps)."""
@@ -106,7 +124,7 @@ class TraceSystem:
 
     def bilu0(self, Hg, Mg, status=None, stream=None):
         if self.pending_mdf:
-            self.set_order(*self.mdf_order(Hg, stream))
+            self.set_levels(*self.mdf_order(Hg, stream))
         Mg.t.copy_(Hg.t)
         st = status.ptr if status is not None else None
         check(lib().hdgx_bilu0_factor(ct.byref(self.bsr), Mg.ptr, st, _stream_ptr(stream)), "hdgx_bilu0_factor")

@@ -23,14 +23,17 @@ def _setup(oracle, name, kw, ordering="multicolor"):
     r = oracle.hdg_elemental(P.master, P.app, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), P.SH)
     Hg, Rg = oracle.globalassembly(P.mesh, r["AE"], r["FE"], P.master.npf, P.app.ncu)
     ts = TraceSystem(P.mesh, P.master, P.app, ordering=ordering)
-    if ordering == "mdf":
+    if ordering in ("mdf", "mdf-flags"):
         o2u, u2o = ts.mdf_order(DArray.from_numpy(Hg))
-        ts.set_order(o2u, u2o)
+        if ordering == "mdf":
+            ts.set_levels(o2u, u2o)
+        else:
+            ts.set_order(o2u, u2o)
     return P, r, Hg, Rg, ts, DArray
 
 
 def _order(ts):
-    if ts.bsr.ncolors == 0:
+    if hasattr(ts, "o2u"):
         return ts.o2u, ts.u2o
     return ts.ord.o2u, ts.ord.u2o
 
@@ -60,7 +63,7 @@ def test_globalassembly_matvec(oracle, name, kw):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("ordering", ["multicolor", "mdf"])
+@pytest.mark.parametrize("ordering", ["multicolor", "mdf", "mdf-flags"])
 @pytest.mark.parametrize("name,kw", CASES)
 def test_bilu0_factor_and_apply_same_order(oracle, name, kw, ordering):
     P, r, Hg, Rg, ts, DArray = _setup(oracle, name, kw, ordering)
@@ -77,7 +80,7 @@ def test_bilu0_factor_and_apply_same_order(oracle, name, kw, ordering):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("ordering", ["multicolor", "mdf"])
+@pytest.mark.parametrize("ordering", ["multicolor", "mdf", "mdf-flags"])
 @pytest.mark.parametrize("name,kw", CASES)
 def test_gmres_solution(oracle, name, kw, ordering):
     P, r, Hg, Rg, ts, DArray = _setup(oracle, name, kw, ordering)

@@ -37,7 +37,9 @@ const char *hdgx_status_str(int code) {
         case -12: return "kernel launch failed";
         case -13: return "CUDA error while counting status";
         case -14: return "a flag-synchronised BILU(0) sweep gave up waiting (bounded spin)";
-        default: return "unknown status";
+        default:
+            if (code <= -1000) return cudaGetErrorString((cudaError_t)(-1000 - code));
+            return "unknown status";
     }
 }
 

@@ -50,10 +50,13 @@ __global__ void bilu0_bwd_bs_kernel(const int *, int, const long long *, const i
 template <int BS>
 __global__ void bsr_matvec_bs_kernel(int, const long long *, const int *, const double *, const double *, double *);
 
+// SM count of the current device (queried each time: host threads of a server may call in
+// concurrently and on different devices)
 static int sm_count() {
-    static int n = 0;
-    if (!n) { int d = 0; cudaGetDevice(&d); cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d); }
-    return n;
+    int d = 0, n = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d);
+    return n > 0 ? n : 1;
 }
 static unsigned grid_for(size_t n, int threads) {
     size_t g = (n + threads - 1) / threads;
@@ -61,7 +64,11 @@ static unsigned grid_for(size_t n, int threads) {
     if (g > cap) g = cap;
     return (unsigned)(g < 1 ? 1 : g);
 }
-static int launched() { return cudaGetLastError() == cudaSuccess ? 0 : -12; }
+// 0, or -1000 - cudaError_t of the last failed call (hdgx_status_str decodes it)
+static int launched() {
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : -1000 - (int)e;
+}
 
 static size_t bilu_smem(int bs) { return sizeof(double) * (4 * (size_t)bs * bs + 200 + 4 + 1); }
 
@@ -180,8 +187,7 @@ int hdgx_bilu0_factor(const hdgx_bsr *A, double *Mg, int *status, hdgx_stream_t 
     if (smem > 200 * 1024) return -3;
     if (A->ncolors == 0) {
         if (!A->sched) return -1;
-        if (cudaFuncSetAttribute(bilu0_sched_factor_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
+        if (allow_dynamic_smem((const void *)bilu0_sched_factor_kernel<NT>, smem) != cudaSuccess)
             return -10;
         const int grid = resident_grid((const void *)bilu0_sched_factor_kernel<NT>, NT, smem, A->nf);
         sched_begin_kernel<<<1, 1, 0, st>>>(A->sched);
@@ -189,7 +195,7 @@ int hdgx_bilu0_factor(const hdgx_bsr *A, double *Mg, int *status, hdgx_stream_t 
                                                               Mg, A->sched, status);
         return launched();
     }
-    if (cudaFuncSetAttribute(bilu0_color_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (allow_dynamic_smem((const void *)bilu0_color_kernel<NT>, smem) != cudaSuccess)
         return -10;
     for (int c = 0; c < A->ncolors; c++) {
         const int r0 = A->color_ptr[c], nr = A->color_ptr[c + 1] - r0;
@@ -221,7 +227,7 @@ int hdgx_block_norms(const hdgx_bsr *A, const double *Hg, double *C, hdgx_stream
     if (!A || !Hg || !C || A->bs > 128) return -1;
     const size_t need = sizeof(double) * (2 * (size_t)A->bs * A->bs + 130 + 8);
     if (need > 227 * 1024) return -3;
-    if (cudaFuncSetAttribute(block_norms_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) != cudaSuccess)
+    if (allow_dynamic_smem((const void *)block_norms_kernel<256>, need) != cudaSuccess)
         return -10;
     const int grid = A->nf < sm_count() * 4 ? A->nf : sm_count() * 4;
     block_norms_kernel<256><<<grid, 256, need, (cudaStream_t)stream>>>(A->bs, A->nf, A->rowpts, Hg, C);
@@ -258,9 +264,10 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
     gs.y = gs.g + (m + 1);
     gs.scal = gs.y + (m + 1);
     double *part = gs.scal + 8;
-    double *h_nrmb = nullptr, *h_res = nullptr;
-    cudaMallocHost(&h_nrmb, sizeof(double) * 2);
-    h_res = h_nrmb + 1;
+    // host scalars on the stack (pageable copies are stream-ordered and, unlike freeing
+    // pinned memory, never synchronise the other streams of the device)
+    double h_scal[2] = {0.0, 0.0};
+    double *h_nrmb = h_scal, *h_res = h_scal + 1;
     int rc = 0;
     // pb = P^{-1} b, nrmb = |pb|
     rc |= bilu0_apply(A, Mg, b, t, pb, st);
@@ -317,7 +324,6 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
         cudaMemcpy(&sched_err, A->sched + 2, sizeof(int), cudaMemcpyDeviceToHost);
         if (sched_err) cudaMemset(A->sched + 2, 0, sizeof(int));
     }
-    cudaFreeHost(h_nrmb);
     if (own) cudaFreeAsync(mem, st);
     if (cudaGetLastError() != cudaSuccess) return -12;
     if (sched_err) return -14;

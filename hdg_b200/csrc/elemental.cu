@@ -791,7 +791,7 @@ static int launch_t(const ElemParams &p, cudaStream_t st) {
     const size_t smem = L::bytes;
     if (smem > 227 * 1024) return -3;
     auto kern = elemental_kernel<D, VISC, MIXED, NT>;
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t err = allow_dynamic_smem((const void *)kern, smem);
     if (err != cudaSuccess) return -10;
     int dev = 0, nsm = 0, per_sm = 0;
     cudaGetDevice(&dev);

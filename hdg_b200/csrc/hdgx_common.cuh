@@ -3,6 +3,29 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "../../include/hdgx.h"
+#include <map>
+#include <mutex>
+#include <utility>
+
+namespace hdgx {
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` on the current device.
+// The limit is a process-wide attribute of the function: host threads that launch the same
+// kernel for different block sizes would otherwise lower it under one another's launches
+// (which then fail with "invalid argument").  The limit only ever grows here, under a lock.
+inline cudaError_t allow_dynamic_smem(const void *fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> granted;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t &g = granted[std::make_pair(dev, fn)];
+    if (bytes <= g) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) g = bytes;
+    return e;
+}
+}  // namespace hdgx
 
 namespace hdgx {
 

@@ -174,7 +174,7 @@ int schur_launch(int qform, int nd, int npv, int ncu, int nc, int ndf, int ne, c
     if (L.bytes > 227 * 1024) return -3;
     p.tile = tile;
     auto kern = schur_kernel<NT>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes) != cudaSuccess) return -10;
+    if (allow_dynamic_smem((const void *)kern, L.bytes) != cudaSuccess) return -10;
     int dev = 0, nsm = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

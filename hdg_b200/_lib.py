@@ -31,7 +31,8 @@ class HdgxApp(ct.Structure):
 
 class HdgxBsr(ct.Structure):
     _fields_ = [("nf", ct.c_int), ("bs", ct.c_int), ("nnzb", ct.c_longlong), ("rowpts", _dp), ("colind", _dp),
-                ("ncolors", ct.c_int), ("color_ptr", _dp), ("color_rows", _dp), ("pos", _dp), ("sched", _dp)]
+                ("ncolors", ct.c_int), ("color_ptr", _dp), ("color_rows", _dp), ("pos", _dp), ("sched", _dp),
+                ("sweep_plan", _dp), ("sweep_maxd", ct.c_int)]
 
 
 class HdgxAssemblyMap(ct.Structure):

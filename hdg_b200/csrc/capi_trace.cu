@@ -104,6 +104,8 @@ static void sweep_color(const hdgx_bsr *A, int dir, const int *rows, int nr, con
                                                                                   A->pos, Mg, in, out);
 }
 
+int level_sweep_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *y, double *v, cudaStream_t st);
+
 static int resident_grid(const void *kern, int threads, size_t smem, int cap) {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
@@ -126,6 +128,7 @@ static int bilu0_apply(const hdgx_bsr *A, const double *Mg, const double *x, dou
         return launched();
     }
     (void)warps;
+    if (A->sweep_plan && level_sweep_apply(A, Mg, x, y, v, st) == 0) return launched();
     for (int c = 0; c < A->ncolors; c++) {
         const int r0 = A->color_ptr[c], nr = A->color_ptr[c + 1] - r0;
         if (nr > 0) sweep_color(A, 0, A->color_rows + r0, nr, Mg, x, y, st);

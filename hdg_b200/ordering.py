@@ -121,3 +121,45 @@ def levels_of_order(rowpts, colind, o2u, u2o):
     ptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
     return Ordering(nlev, ptr, rows, np.asarray(u2o, dtype=np.int32), np.asarray(o2u, dtype=np.int32),
                     np.asarray(u2o, dtype=np.int32))
+
+
+def sweep_plan(order, rowpts, colind):
+    """Flattened level schedule for the single-launch BILU(0) sweeps (hdgx_bsr.sweep_plan):
+    [ncolors+1] level offsets, then per slot q of ``order.color_rows`` the record
+    (row i, diagonal block rowpts[i], maxd (block, column) pairs of the neighbours eliminated
+    before i, maxd pairs of those eliminated after i), -1 padded, 0-based, neighbours in CSR
+    order.  Returns (plan int32 array, maxd), or (None, 0) when a row has more than 6
+    off-diagonal blocks."""
+    rp = np.asarray(rowpts, dtype=np.int64)
+    ci = np.asarray(colind, dtype=np.int64) - 1
+    nf = len(rp) - 1
+    deg = np.diff(rp) - 1
+    dmax = int(deg.max()) if nf else 0
+    if dmax > 6:
+        return None, 0
+    maxd = 4 if dmax <= 4 else 6
+    pos = np.asarray(order.pos, dtype=np.int64)
+    rows = np.asarray(order.color_rows, dtype=np.int64)
+    row_of = np.repeat(np.arange(nf), np.diff(rp))
+    k = np.arange(len(ci))
+    off = k != rp[row_of]
+    k, i, j = k[off], row_of[off], ci[off]
+    later = (pos[j] > pos[i]).astype(np.int64)
+    # rank of each entry inside its (row, earlier/later) group, entries kept in CSR order
+    grp = i * 2 + later
+    srt = np.lexsort((k, grp))
+    g = grp[srt]
+    start = np.r_[0, np.flatnonzero(np.diff(g)) + 1]
+    first = np.repeat(start, np.diff(np.r_[start, len(g)]))
+    rank = np.arange(len(g)) - first
+    RW = 2 + 4 * maxd
+    recs = np.full((nf, RW), -1, dtype=np.int64)
+    slot = np.empty(nf, dtype=np.int64)
+    slot[rows] = np.arange(nf)
+    recs[:, 0] = rows
+    recs[:, 1] = rp[rows]
+    col = 2 + 2 * maxd * later[srt] + 2 * rank
+    recs[slot[i[srt]], col] = k[srt]
+    recs[slot[i[srt]], col + 1] = j[srt]
+    plan = np.concatenate([np.asarray(order.color_ptr, dtype=np.int64), recs.ravel()]).astype(np.int32)
+    return plan, maxd

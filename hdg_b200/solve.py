@@ -22,7 +22,7 @@ import torch
 from ._lib import HdgxAssemblyMap, HdgxBsr, check, lib
 from .elemental import (DArray, DeviceMaster, alloc_elemental_outputs, app_struct, as_darray, _require_cuda,
                         _stream_ptr)
-from .ordering import assembly_map, levels_of_order, multicolor
+from .ordering import assembly_map, levels_of_order, multicolor, sweep_plan
 
 
 class TraceSystem:
@@ -78,6 +78,11 @@ class TraceSystem:
         self.bsr.color_rows = self.d["color_rows"].ptr
         self.bsr.pos = self.d["pos"].ptr
         self.bsr.sched = None
+        plan, maxd = sweep_plan(lv, self.rowpts_h, self.colind_h)
+        if plan is not None:
+            self.d["sweep_plan"] = DArray.from_numpy(plan, dtype=torch.int32)
+            self.bsr.sweep_plan = self.d["sweep_plan"].ptr
+            self.bsr.sweep_maxd = maxd
         self.pending_mdf = False
 
     def set_order(self, o2u, u2o):
@@ -93,6 +98,7 @@ class TraceSystem:
         self.bsr.color_rows = self.d["color_rows"].ptr
         self.bsr.pos = self.d["pos"].ptr
         self.bsr.sched = self.sched.data_ptr()
+        self.bsr.sweep_plan = None
         self.pending_mdf = False
 
     def mdf_order(self, Hg, stream=None):

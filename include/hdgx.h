@@ -128,6 +128,14 @@ typedef struct {
                                   the caller.  Rows are then eliminated one after another in the
                                   order color_rows (e.g. the MDF order of computeMDFordering.m), with
                                   flag-synchronised (not level-synchronised) parallel sweeps. */
+    const int *sweep_plan;     /* optional (NULL: one launch per colour in hdgx_bilu0_apply): the
+                                  colours as levels of a sequential order, for single-launch sweeps.
+                                  Device ints: [ncolors+1] colour offsets, then for every slot q of
+                                  color_rows a record of 2 + 4*sweep_maxd ints: row i, its diagonal
+                                  block rowpts[i], sweep_maxd (block k, column j) pairs of the
+                                  neighbours eliminated before i, sweep_maxd pairs of those eliminated
+                                  after i (k = -1 pads each list; 0-based). */
+    int sweep_maxd;            /* 4 (triangles) or 6 (tetrahedra); other values disable the plan */
 } hdgx_bsr;
 
 /* Element -> block gather map for hdgx_globalassembly (device pointers):

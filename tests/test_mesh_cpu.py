@@ -65,3 +65,29 @@ def test_partition_of_unity_and_quadrature():
         assert np.allclose(ms.shapvl[:, :, 1:].sum(axis=0), 0.0, atol=1e-10)
         vol = 0.5 if nd == 2 else 1.0 / 6.0
         assert abs(ms.gwvl.sum() - vol) < 1e-12
+
+
+def test_sweep_plan_records_match_the_level_schedule():
+    """Every record lists exactly the row's earlier / later neighbours in CSR order."""
+    from hdg_b200.ordering import levels_of_order, sweep_plan
+    m = mkmesh_square(6, 6, 2, 0, 1.0, 1.0)
+    rp, ci = np.asarray(m.cbsr_rowpts), np.asarray(m.cbsr_colind)
+    rng = np.random.default_rng(5)
+    o2u = rng.permutation(m.nf).astype(np.int32)
+    u2o = np.empty_like(o2u)
+    u2o[o2u] = np.arange(m.nf, dtype=np.int32)
+    lv = levels_of_order(rp, ci, o2u, u2o)
+    plan, maxd = sweep_plan(lv, rp, ci)
+    assert maxd == 4
+    assert np.array_equal(plan[:lv.ncolors + 1], lv.color_ptr)
+    recs = plan[lv.ncolors + 1:].reshape(m.nf, 2 + 4 * maxd)
+    for q in range(m.nf):
+        i = lv.color_rows[q]
+        assert recs[q, 0] == i and recs[q, 1] == rp[i]
+        ks = list(range(rp[i] + 1, rp[i + 1]))
+        before = [(k, ci[k] - 1) for k in ks if lv.pos[ci[k] - 1] < lv.pos[i]]
+        after = [(k, ci[k] - 1) for k in ks if lv.pos[ci[k] - 1] > lv.pos[i]]
+        for lst, c0 in ((before, 2), (after, 2 + 2 * maxd)):
+            got = recs[q, c0:c0 + 2 * maxd].reshape(maxd, 2)
+            assert [tuple(x) for x in got[:len(lst)]] == lst
+            assert np.all(got[len(lst):] == -1)

@@ -208,6 +208,7 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-newton", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--n", type=int, default=None, help="squares/cubes per side (smaller profiling cases)")
     args = ap.parse_args()
@@ -368,11 +369,34 @@ def main():
         }
         if not args.no_newton and ws == 1:
             line["newton"] = newton_step(P, torch, args)
+        if not args.no_serve and ws == 1:
+            line["serve"] = serve_mix(torch)
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def serve_mix(torch, count=16, slots=8, ordering="mdf"):
+    """Serving: a seeded stream of independent steady solves (2D, n x n x 2 triangles with
+    n in 8..20, p in 1..4, Mach 0.3-0.8, half Euler / half NS Re 200-2000, Poisson arrivals at
+    20/s) served with continuous admission on per-request streams, against the same requests
+    run back to back; solves/s, p50/p99 latency, and whether every result in the mix equals
+    its result alone bit for bit."""
+    from hdg_b200.serve import Server, request_mix
+    kw = dict(nmin=8, nmax=20, pmin=1, pmax=4, rate=20.0)
+    seq = request_mix(11, count, **kw)
+    s_seq = Server(slots=1, ordering=ordering).serve_sequential(seq)
+    conc = request_mix(11, count, **kw)
+    s_conc = Server(slots=slots, ordering=ordering).serve(conc)
+    same = all(a.UDG is not None and b.UDG is not None and np.array_equal(a.UDG, b.UDG)
+               and np.array_equal(a.UH, b.UH) for a, b in zip(seq, conc))
+    torch.cuda.empty_cache()
+    return {"requests": count, "slots": slots, "ordering": ordering, "newton_tol": 1e-10,
+            "mix": "2D n x n x 2, n 8-20, p 1-4, M 0.3-0.8, half Euler / half NS Re 200-2000, Poisson 20/s (seed 11)",
+            "concurrent": s_conc, "sequential": s_seq, "identical_alone_vs_mix": bool(same),
+            "speedup_solves_per_s": s_conc["solves_per_s"] / s_seq["solves_per_s"]}
 
 
 def newton_step(P, torch, args):

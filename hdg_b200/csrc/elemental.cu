@@ -613,16 +613,15 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     }
                     __syncthreads();
                 }
-            } else if constexpr (VISC) {
-                // the viscous local matrix needs row exchanges (the unpivoted check fails on it)
-                gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
             } else {
-                // fast path: unpivoted elimination; accepted when the backward error of the first
-                // column, |b0 - SD x0| / (|SD| |x0| + |b0|) (infinity norms), is below 1e-13
+                // fast path: unpivoted elimination with the density unknowns last (interior nodes
+                // have structurally zero density pivots in natural order); accepted when the
+                // backward error of the first column, |b0 - SD x0| / (|SD| |x0| + |b0|) (infinity
+                // norms), is below 1e-13, else redone with partial pivoting
                 double *s_b0 = sm + L::d_b0;
                 for (int i = tid; i < NU; i += NT) s_b0[i] = s_R[i];
                 __syncthreads();
-                gj_regs_nopiv<NU, 1 + NH, NT, 8>(s_SD, s_R, s_pcol, s_bad);
+                gj_regs_nopiv<NU, 1 + NH, NT, 8, NPV>(s_SD, s_R, s_pcol, s_bad);
                 {
                     double rmax = 0.0, amax = 0.0, xmax = 0.0, bmax = 0.0;
                     for (int r = tid; r < NU; r += NT) {

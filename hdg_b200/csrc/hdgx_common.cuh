@@ -399,9 +399,13 @@ __device__ __forceinline__ void gj_regs(const double *__restrict__ A, double *B,
 // lane of the next pivot row publishes the next column and the reciprocal of the next
 // pivot at the end of each step.  Used for M (symmetric positive definite) and as the
 // fast path for the local matrix SD, whose result is then checked (backward error) and
-// redone with gj_regs<..., PIVOT = true> when the check fails.  *bad = k+1 for the first
-// zero or non-finite pivot.  Shared scratch: pcol[2N + 2].
-template <typename T, int N, int NR1, int NR2, bool IDENT2, int NT, int TR>
+// redone with gj_regs<..., PIVOT = true> when the check fails.  ROT > 0 eliminates the
+// symmetrically permuted system (P A P^T) (P x) = P B with (P v)[i] = v[(i + ROT) % N]: for
+// the local matrix SD with ROT = npv the density unknowns (component 0) come last, which
+// removes the structurally zero density pivots of interior nodes (the continuity flux does
+// not depend on the density).  Results are returned in natural order.  *bad = k+1 for the
+// first zero or non-finite pivot.  Shared scratch: pcol[2N + 2].
+template <typename T, int N, int NR1, int NR2, bool IDENT2, int NT, int TR, int ROT = 0>
 __device__ __forceinline__ void gj_regs_nopiv_t(const double *__restrict__ A, double *B, double *B2, T *pcol, int *bad) {
     constexpr int NR = NR1 + NR2;
     static_assert(32 % TR == 0 && NT % TR == 0, "TR must divide 32 and NT");
@@ -410,6 +414,7 @@ __device__ __forceinline__ void gj_regs_nopiv_t(const double *__restrict__ A, do
     constexpr int RPT = (N + TR - 1) / TR;
     constexpr int CPT = (NCOL + TC - 1) / TC;
     const int tid = threadIdx.x, tr = tid % TR, tc = tid / TR, lane = tid & 31;
+    auto rot = [](int x) { return ROT == 0 ? x : (x + ROT < N ? x + ROT : x + ROT - N); };
     T a[RPT][CPT];
 #pragma unroll
     for (int i = 0; i < RPT; i++)
@@ -418,9 +423,10 @@ __device__ __forceinline__ void gj_regs_nopiv_t(const double *__restrict__ A, do
             const int r = tr + i * TR, j = tc + jj * TC;
             double v = 0.0;
             if (r < N && j < NCOL) {
-                if (j < N) v = A[r + N * j];
-                else if (j < N + NR1) v = B[r + N * (j - N)];
-                else v = IDENT2 ? ((j - N - NR1 == r) ? 1.0 : 0.0) : B2[r + N * (j - N - NR1)];
+                const int pr = rot(r);
+                if (j < N) v = A[pr + N * rot(j)];
+                else if (j < N + NR1) v = B[pr + N * (j - N)];
+                else v = IDENT2 ? ((j - N - NR1 == pr) ? 1.0 : 0.0) : B2[pr + N * (j - N - NR1)];
             }
             a[i][jj] = (T)v;
         }
@@ -488,16 +494,17 @@ __device__ __forceinline__ void gj_regs_nopiv_t(const double *__restrict__ A, do
             const int r = tr + i * TR, j = tc + jj * TC;
             if (r < N && j >= N && j < NCOL) {
                 const double v = (double)(a[i][jj] / pcol[r]);
-                if (j < N + NR1) B[r + N * (j - N)] = v;
-                else B2[r + N * (j - N - NR1)] = v;
+                const int pr = rot(r);
+                if (j < N + NR1) B[pr + N * (j - N)] = v;
+                else B2[pr + N * (j - N - NR1)] = v;
             }
         }
     __syncthreads();
 }
 
-template <int N, int NR, int NT, int TR>
+template <int N, int NR, int NT, int TR, int ROT = 0>
 __device__ __forceinline__ void gj_regs_nopiv(const double *__restrict__ A, double *B, double *pcol, int *bad) {
-    gj_regs_nopiv_t<double, N, NR, 0, false, NT, TR>(A, B, nullptr, pcol, bad);
+    gj_regs_nopiv_t<double, N, NR, 0, false, NT, TR, ROT>(A, B, nullptr, pcol, bad);
 }
 
 }  // namespace hdgx

@@ -587,15 +587,20 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         {
             int bad_before = *s_bad;
             __syncthreads();
+            // Unpivoted elimination with the density unknowns last (in natural order interior
+            // nodes have structurally zero density pivots: the continuity flux does not depend on
+            // the density), accepted when the backward error of the first column,
+            // |b0 - SD x0| / (|SD| |x0| + |b0|) (infinity norms), is below 1e-13; otherwise the
+            // element is redone with partial pivoting in FP64.
+            double *s_b0 = sm + L::d_b0;
+            for (int i = tid; i < NU; i += NT) s_b0[i] = s_R[i];
+            __syncthreads();
             if constexpr (MIXED) {
-                // FP32 elimination of [SD | R | I]; then refine the residual column in FP64
-                double *s_b0 = sm + L::d_b0;
+                // FP32 elimination of [SD | R | I], then the residual column refined in FP64
+                // against the FP64 SD with the FP32 inverse
                 double *s_inv = sm + L::d_inv;
-                for (int i = tid; i < NU; i += NT) s_b0[i] = s_R[i];
-                __syncthreads();
-                gj_regs_t<float, NU, 1 + NH, NU, true, NT, 8, true>(s_SD, s_R, s_inv, reinterpret_cast<float *>(s_pcol),
-                                                                     reinterpret_cast<float *>(s_diag), s_rowvar,
-                                                                     s_gslot, s_bad);
+                gj_regs_nopiv_t<float, NU, 1 + NH, NU, true, NT, 8, NPV>(s_SD, s_R, s_inv,
+                                                                        reinterpret_cast<float *>(s_pcol), s_bad);
                 double *s_res = s_pcol;                    // free after the elimination
                 for (int it = 0; it < 3; it++) {
                     for (int r = tid; r < NU; r += NT) {
@@ -614,60 +619,53 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     __syncthreads();
                 }
             } else {
-                // fast path: unpivoted elimination with the density unknowns last (interior nodes
-                // have structurally zero density pivots in natural order); accepted when the
-                // backward error of the first column, |b0 - SD x0| / (|SD| |x0| + |b0|) (infinity
-                // norms), is below 1e-13, else redone with partial pivoting
-                double *s_b0 = sm + L::d_b0;
-                for (int i = tid; i < NU; i += NT) s_b0[i] = s_R[i];
-                __syncthreads();
                 gj_regs_nopiv<NU, 1 + NH, NT, 8, NPV>(s_SD, s_R, s_pcol, s_bad);
-                {
-                    double rmax = 0.0, amax = 0.0, xmax = 0.0, bmax = 0.0;
-                    for (int r = tid; r < NU; r += NT) {
-                        double res = s_b0[r], as = 0.0;
-                        for (int c = 0; c < NU; c++) {
-                            const double sd = s_SD[r + NU * c];
-                            res -= sd * s_R[c];
-                            as += fabs(sd);
-                        }
-                        rmax = fmax(rmax, fabs(res));
-                        amax = fmax(amax, as);
-                        xmax = fmax(xmax, fabs(s_R[r]));
-                        bmax = fmax(bmax, fabs(s_b0[r]));
+            }
+            {
+                double rmax = 0.0, amax = 0.0, xmax = 0.0, bmax = 0.0;
+                for (int r = tid; r < NU; r += NT) {
+                    double res = s_b0[r], as = 0.0;
+                    for (int c = 0; c < NU; c++) {
+                        const double sd = s_SD[r + NU * c];
+                        res -= sd * s_R[c];
+                        as += fabs(sd);
                     }
-                    if (!(rmax == rmax)) rmax = INFINITY;
-                    for (int o = 16; o > 0; o >>= 1) {
-                        rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
-                        amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-                        xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
-                        bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
-                    }
-                    double *red = s_pcol;   // free after the elimination
-                    if ((tid & 31) == 0) {
-                        red[4 * (tid >> 5) + 0] = rmax; red[4 * (tid >> 5) + 1] = amax;
-                        red[4 * (tid >> 5) + 2] = xmax; red[4 * (tid >> 5) + 3] = bmax;
-                    }
-                    __syncthreads();
-                    if (tid == 0) {
-                        double R = 0.0, A = 0.0, X = 0.0, B = 0.0;
-                        for (int w = 0; w < NT / 32; w++) {
-                            R = fmax(R, red[4 * w]); A = fmax(A, red[4 * w + 1]);
-                            X = fmax(X, red[4 * w + 2]); B = fmax(B, red[4 * w + 3]);
-                        }
-                        const double den = A * X + B;
-                        const bool ok = (*s_bad == bad_before) && (R <= 1e-13 * den) && isfinite(R);
-                        s_gslot[0] = ok ? 0 : 1;
-                        if (!ok) *s_bad = bad_before;
-                    }
-                    __syncthreads();
+                    rmax = fmax(rmax, fabs(res));
+                    amax = fmax(amax, as);
+                    xmax = fmax(xmax, fabs(s_R[r]));
+                    bmax = fmax(bmax, fabs(s_b0[r]));
                 }
-                if (s_gslot[0]) {
-                    // fall back to partial pivoting on the original system
-                    build_rhs();
-                    __syncthreads();
-                    gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
+                if (!(rmax == rmax)) rmax = INFINITY;
+                for (int o = 16; o > 0; o >>= 1) {
+                    rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+                    amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+                    xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+                    bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
                 }
+                double *red = s_pcol;   // free after the elimination
+                if ((tid & 31) == 0) {
+                    red[4 * (tid >> 5) + 0] = rmax; red[4 * (tid >> 5) + 1] = amax;
+                    red[4 * (tid >> 5) + 2] = xmax; red[4 * (tid >> 5) + 3] = bmax;
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    double R = 0.0, A = 0.0, X = 0.0, B = 0.0;
+                    for (int w = 0; w < NT / 32; w++) {
+                        R = fmax(R, red[4 * w]); A = fmax(A, red[4 * w + 1]);
+                        X = fmax(X, red[4 * w + 2]); B = fmax(B, red[4 * w + 3]);
+                    }
+                    const double den = A * X + B;
+                    const bool ok = (*s_bad == bad_before) && (R <= 1e-13 * den) && isfinite(R);
+                    s_gslot[0] = ok ? 0 : 1;
+                    if (!ok) *s_bad = bad_before;
+                }
+                __syncthreads();
+            }
+            if (s_gslot[0]) {
+                // fall back to partial pivoting on the original system
+                build_rhs();
+                __syncthreads();
+                gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
             }
             if (tid == 0 && *s_bad && !bad_before) *s_bad = 2;
             __syncthreads();
@@ -719,60 +717,72 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         }
 
         // ============ DUDG_DUH and AE = H + GK DUDG_DUH in column tiles (schur_primal.m:136-147)
+        // Each column tile runs four batched small GEMMs with register tiles:
+        //   X   = DUDG_DUH columns: u rows copied from the solve, q rows = MiC dlu - MiE
+        //   Xg  = X at the face Gauss points (shapft through perm), per face
+        //   Y   = Gp Xg, per face Gauss point (GK applied without forming it)
+        //   AE  = shapfg Y (+ the face-block-diagonal H), per face
         {
             constexpr int T = L::TILE;
+            constexpr int TMQ = NPV <= 6 ? NPV : (NPV + 1) / 2;
             double *yX = sm + L::y_X, *yXg = sm + L::y_Xg, *yY = sm + L::y_Y;
             double *g_dd = P.DUDG_DUH + (size_t)e * NQ * NH;
             double *g_ae = P.AE + (size_t)e * NH * NH;
             for (int k0 = 0; k0 < NH; k0 += T) {
                 const int nt = (NH - k0) < T ? (NH - k0) : T;
-                for (int i = tid; i < NQ * nt; i += NT) {
-                    const int rc = i % NQ, t = i / NQ, k = k0 + t;
-                    const int r = rc % NPV, c = rc / NPV;
-                    const double *dlu = s_R + NU * (1 + k);
-                    double v;
-                    if (c < NCU) {
-                        v = dlu[r + NPV * c];
-                    } else {
-                        const int a = (c - NCU) % NCU, d = (c - NCU) / NCU;
-                        const int b = k % NCU, f = k / NCU;
-                        v = (a == b) ? -s_MiE[r + NPV * (f + NDF * d)] : 0.0;
-#pragma unroll
-                        for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * dlu[s + NPV * a];
-                    }
-                    yX[i] = v;
-                    g_dd[(size_t)NQ * k0 + i] = v;
+                for (int i = tid; i < NU * nt; i += NT) {
+                    const int ru = i % NU, t = i / NU;
+                    const double v = s_R[NU * (1 + k0 + t) + ru];
+                    yX[ru + NQ * t] = v;
+                    g_dd[(size_t)NQ * (k0 + t) + ru] = v;
                 }
+                // q rows r + NPV (NCU + a + NCU d) of column k = k0 + t, batch d, n = (a, t)
+                tile_gemm<ND, NPV, NCU * T, NPV, TMQ, 2, NT>(
+                    [&](int d, int r, int sx) { return s_MiC[r + NPV * (sx + NPV * d)]; },
+                    [&](int, int sx, int n) {
+                        const int t = n / NCU;
+                        return t < nt ? s_R[NU * (1 + k0) + sx + NPV * n] : 0.0;
+                    },
+                    [&](int d, int r, int n, double v) {
+                        const int a = n % NCU, t = n / NCU;
+                        if (t >= nt) return;
+                        const int k = k0 + t;
+                        if (a == k % NCU) v -= s_MiE[r + NPV * (k / NCU + NDF * d)];
+                        const int row = r + NPV * (NCU + a + NCU * d);
+                        yX[row + NQ * t] = v;
+                        g_dd[(size_t)NQ * k + row] = v;
+                    });
                 __syncthreads();
-                for (int i = tid; i < NGT * NCG * nt; i += NT) {
-                    const int gg = i % NGT, c = (i / NGT) % NCG, t = i / (NGT * NCG);
-                    const int g = gg % NGF, j = gg / NGF;
-                    double v = 0.0;
-#pragma unroll
-                    for (int m = 0; m < NPF; m++) v += t_ft[g + NGF * m] * yX[perm[m + NPF * j] + NPV * c + NQ * t];
-                    yXg[i] = v;
-                }
+                // Xg(gg, c, t) = sum_m shapft(g, m) X(perm(m, j), c, t), batch j, n = (c, t)
+                tile_gemm<NFE, NGF, NCG * T, NPF, NGF, 2, NT>(
+                    [&](int, int g, int m) { return t_ft[g + NGF * m]; },
+                    [&](int j, int m, int n) {
+                        const int c = n % NCG, t = n / NCG;
+                        return yX[perm[m + NPF * j] + NPV * c + NQ * t];
+                    },
+                    [&](int j, int g, int n, double v) { yXg[g + NGF * j + NGT * n] = v; });
                 __syncthreads();
-                for (int i = tid; i < NGT * NCU * nt; i += NT) {
-                    const int gg = i % NGT, a = (i / NGT) % NCU, t = i / (NGT * NCU);
-                    double v = 0.0;
-                    for (int c = 0; c < NCG; c++) v += s_Gp[gg + NGT * (a + NCU * c)] * yXg[gg + NGT * (c + NCG * t)];
-                    yY[i] = v;
-                }
+                // Y(gg, a, t) = sum_c Gp(gg, a, c) Xg(gg, c, t), batch gg
+                tile_gemm<NGT, NCU, T, NCG, 2, 2, NT>(
+                    [&](int gg, int a, int c) { return s_Gp[gg + NGT * (a + NCU * c)]; },
+                    [&](int gg, int c, int t) { return yXg[gg + NGT * (c + NCG * t)]; },
+                    [&](int gg, int a, int t, double v) { yY[gg + NGT * (a + NCU * t)] = v; });
                 __syncthreads();
-                for (int i = tid; i < NH * nt; i += NT) {
-                    const int row = i % NH, t = i / NH, k = k0 + t;
-                    const int a = row % NCU, nf = row / NCU, n = nf % NPF, j = nf / NPF;
-                    const int b = k % NCU, fk = k / NCU, nk = fk % NPF, jk = fk / NPF;
-                    double v = 0.0;
-                    for (int g = 0; g < NGF; g++) {
-                        const int gg = g + NGF * j;
-                        double y = yY[gg + NGT * (a + NCU * t)];
-                        if (jk == j) y += t_ft[g + NGF * nk] * s_Hp[gg + NGT * (a + NCU * b)];
-                        v += t_fg[n + NPF * g] * y;
-                    }
-                    g_ae[(size_t)NH * k0 + i] = v;
-                }
+                // AE((a, n, j), k) = sum_g shapfg(n, g) (Y(gg, a, t) + [face of k == j] shapft(g, nk) Hp(gg, a, b)),
+                // batch j, rows n, columns (a, t)
+                tile_gemm<NFE, NPF, NCU * T, NGF, 2, 2, NT>(
+                    [&](int, int n, int g) { return t_fg[n + NPF * g]; },
+                    [&](int j, int g, int nn) {
+                        const int a = nn % NCU, t = nn / NCU, gg = g + NGF * j;
+                        double y = yY[gg + NGT * nn];
+                        const int k = k0 + t, b = k % NCU, fk = k / NCU, nk = fk % NPF, jk = fk / NPF;
+                        if (t < nt && jk == j) y += t_ft[g + NGF * nk] * s_Hp[gg + NGT * (a + NCU * b)];
+                        return y;
+                    },
+                    [&](int j, int n, int nn, double v) {
+                        const int a = nn % NCU, t = nn / NCU;
+                        if (t < nt) g_ae[(size_t)NH * (k0 + t) + a + NCU * (n + NPF * j)] = v;
+                    });
                 __syncthreads();
             }
         }

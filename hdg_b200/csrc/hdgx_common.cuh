@@ -507,4 +507,40 @@ __device__ __forceinline__ void gj_regs_nopiv(const double *__restrict__ A, doub
     gj_regs_nopiv_t<double, N, NR, 0, false, NT, TR, ROT>(A, B, nullptr, pcol, bad);
 }
 
+// Batched small GEMM with register tiles, spread over the NT threads of a CTA:
+//   for b < NB, m < M, n < N:  store(b, m, n, sum_{k < K} a(b, m, k) * bb(b, k, n))
+// Each thread owns TM x TN outputs of one batch entry, so every loaded value feeds TN (or
+// TM) multiply-adds; a(...) / bb(...) return the operands (usually shared-memory reads) and
+// store(...) consumes each result.  Threads are laid out m-tile fastest.
+template <int NB, int M, int N, int K, int TM, int TN, int NT, class FA, class FB, class FS>
+__device__ __forceinline__ void tile_gemm(FA a, FB bb, FS store) {
+    constexpr int MT = (M + TM - 1) / TM, NTL = (N + TN - 1) / TN;
+    for (int t = threadIdx.x; t < NB * MT * NTL; t += NT) {
+        const int mt = t % MT, nt = (t / MT) % NTL, b = t / (MT * NTL);
+        const int m0 = mt * TM, n0 = nt * TN;
+        double acc[TM][TN];
+#pragma unroll
+        for (int i = 0; i < TM; i++)
+#pragma unroll
+            for (int j = 0; j < TN; j++) acc[i][j] = 0.0;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            double av[TM], bv[TN];
+#pragma unroll
+            for (int i = 0; i < TM; i++) av[i] = (M % TM == 0 || m0 + i < M) ? a(b, m0 + i, k) : 0.0;
+#pragma unroll
+            for (int j = 0; j < TN; j++) bv[j] = (N % TN == 0 || n0 + j < N) ? bb(b, k, n0 + j) : 0.0;
+#pragma unroll
+            for (int i = 0; i < TM; i++)
+#pragma unroll
+                for (int j = 0; j < TN; j++) acc[i][j] += av[i] * bv[j];
+        }
+#pragma unroll
+        for (int i = 0; i < TM; i++)
+#pragma unroll
+            for (int j = 0; j < TN; j++)
+                if ((M % TM == 0 || m0 + i < M) && (N % TN == 0 || n0 + j < N)) store(b, m0 + i, n0 + j, acc[i][j]);
+    }
+}
+
 }  // namespace hdgx

@@ -469,40 +469,46 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         __syncthreads();
 
         // ========================= SD = D + B Mi C (schur_primal.m:93-110 with volint/faceint)
-        for (int i = tid; i < NU * NU; i += NT) {
-            const int r = i % NPV, a = (i / NPV) % NCU, k = (i / NU) % NPV, b = i / (NU * NPV);
-            double v = 0.0;
-            for (int g = 0; g < NGV; g++) {
-                const double svk = t_vt[g + NGV * k];
-#pragma unroll
-                for (int id = 0; id < ND; id++) {
-                    double w = x_wrl[g + NGV * (id + ND * (a + NCU * b))] * svk;
+        // One batched GEMM per (a, b) component pair over the volume (g, id) and face (j, g)
+        // quadrature points kk:  SD((r,a),(k,b)) = sum_kk Phi(r, kk) W_ab(kk, k), with
+        //   Phi = shapvg(r, g, id) (volume) / shapfg(m(r, j), g) (face; 0 off the face) and
+        //   W_ab = wrl(g,id,a,b) shapvt(g,k) + sum_d wrl(g,id,a,(b,d)) Zc(g,k,d)           (volume)
+        //        = shapft(g,n(k,j)) FHu(gg,a,b) + sum_d FHu(gg,a,(b,d)) ZFc(gg,k,d)        (face)
+        // W is formed on the fly, once per register tile.
+        constexpr int KV = NGV * ND, KK = KV + NFE * NGF;
+        constexpr int TMS = NPV <= 6 ? NPV : (NPV + 1) / 2;
+        auto phi = [&](int, int r, int kk) -> double {
+            if (kk < KV) return t_vg[r + NPV * (kk + NGV)];      // shapvg(r, g, id + 1), kk = g + NGV id
+            const int kf = kk - KV, j = kf / NGF, g = kf % NGF, m = invp[r + NPV * j];
+            return m >= 0 ? t_fg[m + NPF * g] : 0.0;
+        };
+        tile_gemm<NCU * NCU, NPV, NPV, KK, TMS, 2, NT, 2>(
+            phi,
+            [&](int ab, int kk, int k) -> double {
+                const int a = ab % NCU, b = ab / NCU;
+                if (kk < KV) {
+                    const int g = kk % NGV, id = kk / NGV;
+                    double w = x_wrl[g + NGV * (id + ND * (a + NCU * b))] * t_vt[g + NGV * k];
                     if constexpr (VISC) {
 #pragma unroll
                         for (int d = 0; d < ND; d++)
                             w += x_wrl[g + NGV * (id + ND * (a + NCU * (NCU + b + NCU * d)))] * x_Zc[g + NGV * (k + NPV * d)];
                     }
-                    v += t_vg[r + NPV * (g + NGV * (id + 1))] * w;
+                    return w;
                 }
-            }
+                const int kf = kk - KV, j = kf / NGF, g = kf % NGF, gg = g + NGF * j, nk = invp[k + NPV * j];
+                double w = nk >= 0 ? t_ft[g + NGF * nk] * x_FHu[gg + NGT * (a + NCU * b)] : 0.0;
+                if constexpr (VISC) {
 #pragma unroll
-            for (int j = 0; j < NFE; j++) {
-                const int m = invp[r + NPV * j];
-                if (m < 0) continue;
-                const int nk = invp[k + NPV * j];
-                for (int g = 0; g < NGF; g++) {
-                    const int gg = g + NGF * j;
-                    double w = (nk >= 0) ? t_ft[g + NGF * nk] * x_FHu[gg + NGT * (a + NCU * b)] : 0.0;
-                    if constexpr (VISC) {
-#pragma unroll
-                        for (int d = 0; d < ND; d++)
-                            w += x_FHu[gg + NGT * (a + NCU * (NCU + b + NCU * d))] * x_ZFc[gg + NGT * (k + NPV * d)];
-                    }
-                    v += t_fg[m + NPF * g] * w;
+                    for (int d = 0; d < ND; d++)
+                        w += x_FHu[gg + NGT * (a + NCU * (NCU + b + NCU * d))] * x_ZFc[gg + NGT * (k + NPV * d)];
                 }
-            }
-            s_SD[i] = v;
-        }
+                return w;
+            },
+            [&](int ab, int r, int k, double v) {
+                const int a = ab % NCU, b = ab / NCU;
+                s_SD[(r + NPV * a) + NU * (k + NPV * b)] = v;
+            });
         auto build_rhs = [&]() {
         // rhs0 = Ru - B Mi Rq (volint.m:258, faceint.m:306-331; schur_primal.m:95,111)
         for (int i = tid; i < NU; i += NT) {
@@ -534,44 +540,39 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             }
             s_R[i] = v;
         }
-        // RHS(:, (b,f)) = B Mi E - F   (schur_primal.m:98,118; faceint.m:319-333)
-        for (int i = tid; i < NU * NH; i += NT) {
-            const int r = i % NPV, a = (i / NPV) % NCU, b = (i / NU) % NCU, f = i / (NU * NCU);
-            const int nf = f % NPF, jf = f / NPF;
-            double v = 0.0;
-            if constexpr (VISC) {
-                for (int g = 0; g < NGV; g++)
+        // RHS((r,a), (b,f)) = B Mi E - F   (schur_primal.m:98,118; faceint.m:319-333): the same
+        // batched GEMM with W_ab(kk, f) = sum_d wrl(g,id,a,(b,d)) Ze(g,f,d) (volume) and
+        // sum_d FHu(gg,a,(b,d)) ZFe(gg,f,d) (face), minus the face-block F term
+        tile_gemm<NCU * NCU, NPV, NDF, (VISC ? KK : 0), TMS, 2, NT, 2>(
+            phi,
+            [&](int ab, int kk, int f) -> double {
+                const int a = ab % NCU, b = ab / NCU;
+                double w = 0.0;
+                if (kk < KV) {
+                    const int g = kk % NGV, id = kk / NGV;
 #pragma unroll
-                    for (int id = 0; id < ND; id++) {
-                        double w = 0.0;
+                    for (int d = 0; d < ND; d++)
+                        w += x_wrl[g + NGV * (id + ND * (a + NCU * (NCU + b + NCU * d)))] * x_Ze[g + NGV * (f + NDF * d)];
+                } else {
+                    const int kf = kk - KV, j = kf / NGF, g = kf % NGF, gg = g + NGF * j;
 #pragma unroll
-                        for (int d = 0; d < ND; d++)
-                            w += x_wrl[g + NGV * (id + ND * (a + NCU * (NCU + b + NCU * d)))] * x_Ze[g + NGV * (f + NDF * d)];
-                        v += t_vg[r + NPV * (g + NGV * (id + 1))] * w;
-                    }
-#pragma unroll
-                for (int j = 0; j < NFE; j++) {
-                    const int m = invp[r + NPV * j];
-                    if (m < 0) continue;
-                    for (int g = 0; g < NGF; g++) {
-                        const int gg = g + NGF * j;
-                        double w = 0.0;
-#pragma unroll
-                        for (int d = 0; d < ND; d++)
-                            w += x_FHu[gg + NGT * (a + NCU * (NCU + b + NCU * d))] * x_ZFe[gg + NGT * (f + NDF * d)];
-                        v += t_fg[m + NPF * g] * w;
-                    }
+                    for (int d = 0; d < ND; d++)
+                        w += x_FHu[gg + NGT * (a + NCU * (NCU + b + NCU * d))] * x_ZFe[gg + NGT * (f + NDF * d)];
                 }
-            }
-            const int mf = invp[r + NPV * jf];
-            if (mf >= 0) {
-                double t = 0.0;
-                for (int g = 0; g < NGF; g++)
-                    t += t_fg[mf + NPF * g] * t_ft[g + NGF * nf] * x_FHh[(g + NGF * jf) + NGT * (a + NCU * b)];
-                v -= t;
-            }
-            s_R[NU + i] = v;
-        }
+                return w;
+            },
+            [&](int ab, int r, int f, double v) {
+                const int a = ab % NCU, b = ab / NCU, nf = f % NPF, jf = f / NPF;
+                const int mf = invp[r + NPV * jf];
+                if (mf >= 0) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int g = 0; g < NGF; g++)
+                        t += t_fg[mf + NPF * g] * t_ft[g + NGF * nf] * x_FHh[(g + NGF * jf) + NGT * (a + NCU * b)];
+                    v -= t;
+                }
+                s_R[NU + (r + NPV * a) + NU * (b + NCU * f)] = v;
+            });
         };
         build_rhs();
         // Rh = -(fbou or fhat) integrated on each face (faceint.m:335-339)

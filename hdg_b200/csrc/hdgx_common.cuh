@@ -511,8 +511,9 @@ __device__ __forceinline__ void gj_regs_nopiv(const double *__restrict__ A, doub
 //   for b < NB, m < M, n < N:  store(b, m, n, sum_{k < K} a(b, m, k) * bb(b, k, n))
 // Each thread owns TM x TN outputs of one batch entry, so every loaded value feeds TN (or
 // TM) multiply-adds; a(...) / bb(...) return the operands (usually shared-memory reads) and
-// store(...) consumes each result.  Threads are laid out m-tile fastest.
-template <int NB, int M, int N, int K, int TM, int TN, int NT, class FA, class FB, class FS>
+// store(...) consumes each result.  Threads are laid out m-tile fastest.  UK is the unroll
+// factor of the k loop (K = fully unrolled: every k a compile-time constant).
+template <int NB, int M, int N, int K, int TM, int TN, int NT, int UK = K, class FA, class FB, class FS>
 __device__ __forceinline__ void tile_gemm(FA a, FB bb, FS store) {
     constexpr int MT = (M + TM - 1) / TM, NTL = (N + TN - 1) / TN;
     for (int t = threadIdx.x; t < NB * MT * NTL; t += NT) {
@@ -523,7 +524,7 @@ __device__ __forceinline__ void tile_gemm(FA a, FB bb, FS store) {
         for (int i = 0; i < TM; i++)
 #pragma unroll
             for (int j = 0; j < TN; j++) acc[i][j] = 0.0;
-#pragma unroll
+#pragma unroll UK
         for (int k = 0; k < K; k++) {
             double av[TM], bv[TN];
 #pragma unroll

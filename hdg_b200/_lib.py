@@ -99,6 +99,16 @@ def _declare(L):
     L.hdgx_gmres_bilu0_noalloc.argtypes = [B, v, v, v, v, i, d, i, p(i), p(i), p(d), v, v]
     L.hdgx_backsub.restype = i
     L.hdgx_backsub.argtypes = [i, i, i, i, i, v, v, v, v, v, v]
+    L.hdgx_arraymul.restype = i
+    L.hdgx_arraymul.argtypes = [i, i, i, i, i, i, v, v, v, v]
+    L.hdgx_dense_block_system.restype = i
+    L.hdgx_dense_block_system.argtypes = [B, v, v, i, v, v, v, v, v]
+    L.hdgx_dense_matvec.restype = i
+    L.hdgx_dense_matvec.argtypes = [i, i, i, v, v, v, v, v]
+    L.hdgx_gmres_dense_workspace_bytes.restype = ct.c_size_t
+    L.hdgx_gmres_dense_workspace_bytes.argtypes = [i, i, i]
+    L.hdgx_gmres_dense.restype = i
+    L.hdgx_gmres_dense.argtypes = [i, i, i, v, v, v, v, i, d, i, p(i), p(i), p(d), v, v, v]
     _declare_optional(L)
 
 

@@ -37,6 +37,7 @@ class App:
     tdep: int = 0
     getdqdg: int = 1
     name: str = "ns"
+    denseblock: int = 0               # hdg_solve.m:43-45: 1 = dense face-block GMRES (gmres.m)
 
     @property
     def ncu(self):

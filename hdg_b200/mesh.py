@@ -228,6 +228,28 @@ def block_crs(t2f):
     return rowpts, np.array(cols, dtype=np.int64)
 
 
+def mkf2f(f, t2f):
+    """mesh/mkmesh/mkf2f.m: face-to-face connectivity ``f2f[nbf, nf]`` (1-based, 0 = none),
+    nbf = 2 nfe - 1.  Column i lists face i, then the other faces of its first element, then
+    those of its second element (interior faces only), in local face order."""
+    nf = f.shape[0]
+    nfe = t2f.shape[1]
+    nbf = 2 * nfe - 1
+    f2f = np.zeros((nbf, nf), dtype=np.int64)
+    t2fa = np.abs(np.asarray(t2f))
+    for i in range(nf):
+        e1, e2 = int(f[i, -2]), int(f[i, -1])
+        k = 0
+        f2f[k, i] = i + 1
+        for e in ((e1, e2) if e2 > 0 else (e1,)):
+            kf = t2fa[e - 1]
+            for j in kf:
+                if j != i + 1:
+                    k += 1
+                    f2f[k, i] = j
+    return f2f
+
+
 def mkmesh(p, t, porder, bndexpr, nd):
     """mesh/mkmesh/mkmesh.m + the connectivity part of util/preprocess.m."""
     f, t2f, _ = mkt2f(t, nd)

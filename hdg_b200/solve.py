@@ -168,7 +168,9 @@ class SolveReport:
 class HDGSolver:
     """Device-resident state of one steady problem (mesh, master, app) for Newton steps."""
 
-    def __init__(self, master, mesh, app, ordering=None, restart=20, mixed=False):
+    def __init__(self, master, mesh, app, ordering=None, restart=20, mixed=False, denseblock=False):
+        """denseblock=True solves each Newton step's linear system as the reference does with
+        app.denseblock = 1: mkDenseBlockSystem.m's scaled face blocks and gmres.m (no BILU(0))."""
         _require_cuda()
         self.master, self.mesh, self.app = master, mesh, app
         self.mixed = mixed
@@ -189,7 +191,13 @@ class HDGSolver:
         self.DUDGT = DArray.empty((master.npv, app.nc, ne))
         self.app_c = app_struct(app)
         self.restart = restart
-        self.ws = self.ts.workspace(restart)
+        self.denseblock = denseblock
+        if denseblock:
+            from .dense import DenseBlockSystem
+            self.dense = DenseBlockSystem(self.ts, mesh)
+            self.ws = None
+        else:
+            self.ws = self.ts.workspace(restart)
 
     def gather(self, UH, stream=None):
         ndf = self.master.npf * self.master.nfe
@@ -210,9 +218,12 @@ class HDGSolver:
         return float(torch.linalg.vector_norm(self.Rg.t).item())
 
     def linear_solve(self, tol=1e-10, maxit=1000, stream=None):
-        """DUH = K \\ F with BILU(0)-GMRES (x0 = 0)."""
-        self.ts.bilu0(self.Hg, self.Mg, stream=stream)
+        """DUH = K \\ F with BILU(0)-GMRES, or with the dense face-block GMRES (x0 = 0)."""
         self.DUH.t.zero_()
+        if self.denseblock:
+            self.dense.build(self.Hg, self.Rg, stream)
+            return self.dense.gmres(self.DUH, restart=self.restart, tol=tol, maxit=maxit, stream=stream)
+        self.ts.bilu0(self.Hg, self.Mg, stream=stream)
         return self.ts.gmres(self.Hg, self.Mg, self.Rg, self.DUH, self.restart, tol, maxit, self.ws, stream)
 
     def backsub(self, stream=None):
@@ -269,10 +280,14 @@ class HDGSolver:
 
 
 def hdg_solve(master, mesh, app, UDG, UH, SH=None, tol=1e-10, maxiter=16, gmres_tol=1e-10, restart=20,
-              ordering=None, mixed=False):
+              ordering=None, mixed=False, denseblock=None):
     """kernel/hdg_solve.m: returns (UDG, UH, report) as host arrays (inputs are not modified).
-    ``mixed=True`` assembles with the mixed-precision elemental kernel."""
-    s = HDGSolver(master, mesh, app, ordering=ordering, restart=restart, mixed=mixed)
+    ``mixed=True`` assembles with the mixed-precision elemental kernel; ``denseblock`` (default
+    ``app.denseblock`` when the app has it) selects the dense face-block GMRES of
+    hdg_solve.m:88-92,110-116 instead of BILU(0)-GMRES."""
+    if denseblock is None:
+        denseblock = bool(getattr(app, "denseblock", 0))
+    s = HDGSolver(master, mesh, app, ordering=ordering, restart=restart, mixed=mixed, denseblock=denseblock)
     dU = DArray.from_numpy(UDG)
     dH = DArray.from_numpy(UH)
     dS = DArray.from_numpy(np.zeros_like(UDG) if SH is None else SH)

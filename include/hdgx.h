@@ -22,6 +22,10 @@
  *   hdgx_gmres_bilu0      kernel/gmres_bilu0.m:1     [x,flags,iter,rev] = gmres_bilu0(mesh,M,A,b,x,restart,tol,maxit)
  *   hdgx_backsub          kernel/hdg_solve.m:119-121 DUDGT = DUDG + mapContractK(DUDG_DUH, DUH(elcon))
  *   hdgx_gather_uh        kernel/hdg_assemble.m:34   uh = reshape(UH(:,elcon),[ncu npf*nfe ne])
+ *   hdgx_arraymul         kernel/arraymul.c:11       C = arraymul(A,B)
+ *   hdgx_dense_block_system kernel/mkDenseBlockSystem.m:9  [K,F] = mkDenseBlockSystem(AE,FE,f,t2f,elcon)
+ *   hdgx_dense_matvec     kernel/gmres.m:40-44       d = x + arraymul(K, gather(x, f2f))
+ *   hdgx_gmres_dense      kernel/gmres.m:1           [x,flags,iter,rev] = gmres(K,F,f2f,x,restart,tol,maxit)
  */
 #ifndef HDGX_H
 #define HDGX_H
@@ -207,6 +211,42 @@ int hdgx_gmres_bilu0_noalloc(const hdgx_bsr *A, const double *Hg, const double *
  * DUH[ncu, nsiz]. */
 int hdgx_backsub(int npv, int nc, int ncu, int ndf, int ne, const int *elcon, const double *DUDG,
                  const double *DUDG_DUH, const double *DUH, double *DUDGT, hdgx_stream_t stream);
+
+/* ------------------------------------------------- dense face-block path (app.denseblock = 1) */
+
+/* Batched product (kernel/arraymul.c:11-96).  A is rowsA x colsA x ndim3 (ndim3 = 1 for a 2-D
+ * A).  When B is 2-D (ndimB == 2) with colsB == ndim3: C(:, i) = A(:, :, i) B(:, i), C is
+ * rowsA x ndim3 (batched GEMV).  Otherwise C(:, :, i) = A(:, :, i) B(:, :, i) with B holding
+ * ndim3 rowsB x colsB matrices and C rowsA x colsB x ndim3.  colsA != rowsB -> -1 (the MEX's
+ * "Number of columns of A must be equal to numbers of rows B"). */
+int hdgx_arraymul(int rowsA, int colsA, int ndim3, int rowsB, int colsB, int ndimB, const double *A,
+                  const double *B, double *C, hdgx_stream_t stream);
+
+/* Block-Jacobi-scaled face blocks (kernel/mkDenseBlockSystem.m:9-95) from the block-CSR
+ * condensed system: for face i, K(:, :, k, i) = inv(D_i) H(i, f2f(k+1, i)) (zero block where
+ * f2f(k+1, i) == 0) and F(:, i) = inv(D_i) Rg(:, i), D_i the diagonal block.  f2f[nbf, nf]
+ * (mesh/mkmesh/mkf2f.m, 1-based, 0 = none; row 0 is the face itself).  K[bs, bs*(nbf-1), nf],
+ * F[bs, nf].  status[nf] (optional): k+1 when D_i's pivot k is zero or not finite. */
+int hdgx_dense_block_system(const hdgx_bsr *A, const double *Hg, const double *Rg, int nbf, const int *f2f,
+                            double *K, double *F, int *status, hdgx_stream_t stream);
+
+/* y = x + K gather(x, f2f) (kernel/gmres.m:40-44): y(:, i) = x(:, i) + sum_k K(:, :, k, i) x(:, f2f(k+1, i)). */
+int hdgx_dense_matvec(int nb, int nf, int nbf, const double *K, const int *f2f, const double *x, double *y,
+                      hdgx_stream_t stream);
+
+/* Bytes of device workspace hdgx_gmres_dense uses for a given restart length. */
+size_t hdgx_gmres_dense_workspace_bytes(int nb, int nf, int restart);
+
+/* Unpreconditioned restarted GMRES on (I + K gather) x = b with classical Gram-Schmidt
+ * (kernel/gmres.m:1-111).  x (in: initial guess, out: solution) [nb, nf].  Stops when the
+ * least-squares residual |b - A x| <= tol |b| or after maxit iterations, counted as gmres.m
+ * counts them (each restart's residual evaluation is one).  iters, flag (0 converged,
+ * 1 maxit, 3 breakdown to a non-finite value), relres and history[maxit] (optional, relative
+ * residuals) are host outputs.  workspace (device, hdgx_gmres_dense_workspace_bytes) may be
+ * NULL, in which case it is taken from the stream-ordered allocator. */
+int hdgx_gmres_dense(int nb, int nf, int nbf, const double *K, const int *f2f, const double *b, double *x,
+                     int restart, double tol, int maxit, int *iters, int *flag, double *relres, double *history,
+                     void *workspace, hdgx_stream_t stream);
 
 #ifdef __cplusplus
 }

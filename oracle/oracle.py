@@ -312,3 +312,50 @@ def hdg_solve(P, o2u=None, u2o=None, tol=1e-10, maxiter=16, gmres_tol=1e-10, res
         res.append(F)
         rel = F / F0
     return UDG, UH, res, gits, alphas
+
+
+def dense_block_system(mesh, AE, FE, npf, ncu):
+    """mkf2f.m + mkDenseBlockSystem.m (from the elemental arrays): (f2f, K, F)."""
+    L = lib()
+    ne, nfe = mesh.t2f.shape
+    nf = mesh.nf
+    nbf = 2 * nfe - 1
+    ncf = ncu * npf
+    fel = np.ascontiguousarray(np.asarray(mesh.f)[:, -2:], dtype=np.int32).ravel()
+    f2f = np.zeros((nbf, nf), dtype=np.int32, order="F")
+    K = np.zeros((ncf, ncf * (nbf - 1), nf), order="F")
+    F = np.zeros((ncf, nf), order="F")
+    t2f, el = _i32(np.abs(mesh.t2f)), _i32(mesh.elcon)
+    L.orc_dense_block_system.restype = ct.c_int
+    nbad = L.orc_dense_block_system(ne, nfe, npf, ncu, nf, fel.ctypes.data_as(_ip), t2f.ctypes.data_as(_ip),
+                                    el.ctypes.data_as(_ip), _p(_f(AE)), _p(_f(FE)), f2f.ctypes.data_as(_ip),
+                                    _p(K), _p(F))
+    if nbad:
+        raise RuntimeError(f"{nbad} singular diagonal blocks")
+    return f2f, K, F
+
+
+def dense_matvec(K, f2f, x):
+    L = lib()
+    nb, nf = x.shape
+    nbf = f2f.shape[0]
+    y = np.zeros((nb, nf), order="F")
+    f2 = _i32(f2f)
+    L.orc_dense_matvec(nb, nf, nbf, _p(_f(K)), f2.ctypes.data_as(_ip), _p(_f(x)), _p(y))
+    return y
+
+
+def gmres_dense(K, F, f2f, x0=None, restart=20, tol=1e-6, maxit=None):
+    """kernel/gmres.m: returns (x, flag, iterations, relative residual history)."""
+    L = lib()
+    nb, nf = F.shape
+    nbf = f2f.shape[0]
+    maxit = nb * nf if maxit is None else maxit
+    x = np.zeros((nb, nf), order="F") if x0 is None else np.array(x0, dtype=np.float64, order="F")
+    rev = np.zeros(maxit)
+    flag = ct.c_int(0)
+    f2 = _i32(f2f)
+    L.orc_gmres_dense.restype = ct.c_int
+    it = L.orc_gmres_dense(nb, nf, nbf, _p(_f(K)), f2.ctypes.data_as(_ip), _p(_f(F)), _p(x), int(restart),
+                           ct.c_double(tol), int(maxit), ct.byref(flag), _p(rev))
+    return x, flag.value, it, rev[:it]

@@ -16,6 +16,9 @@
  *                       modified Gram-Schmidt; the Hessenberg least-squares problem
  *                       y = H \ (beta e1) is solved with Givens rotations, which gives the
  *                       same minimiser and residual)
+ *   orc_dense_block_system  mesh/mkmesh/mkf2f.m + kernel/mkDenseBlockSystem.m:9-95
+ *   orc_dense_matvec        kernel/gmres.m:40-44
+ *   orc_gmres_dense         kernel/gmres.m:1-111 (classical Gram-Schmidt)
  * Index conventions: rowpts 0-based offsets [nf+1], colind 1-based [nnzb], diagonal first;
  * elcon [npf*nfe, ne] 1-based; t2f [ne, nfe] 1-based (column-major); orderings 0-based.
  */
@@ -342,4 +345,182 @@ void orc_backsub(int ne, int npv, int nc, int ncu, int ndf, const int *elcon, co
             }
         }
     }
+}
+
+/* ------------------------------------------------------------------ dense face-block path */
+
+/* mesh/mkmesh/mkf2f.m + kernel/mkDenseBlockSystem.m:9-95 (mkBlockSystem1) restated from the
+ * elemental arrays.  fel[2*nf]: the two elements of every face (1-based; <= 0 for none,
+ * f(:,end-1:end)); t2f [ne, nfe] 1-based column-major; elcon [npf*nfe, ne] 1-based.
+ * Outputs f2f [nbf, nf] (1-based, 0 = none), K [ncf, ncf*(nbf-1), nf], F [ncf, nf] with
+ * ncf = ncu*npf, nbf = 2*nfe - 1.  The face blocks are read from AE with the face-local node
+ * index j(n) = elcon(n, a, e) - (i-1)*npf used as an index into AE's face nodes, as
+ * mkDenseBlockSystem.m:45-74 does (equal to the placement by elcon when j is its own
+ * inverse, which holds for the two orientations of a 2D face).  Each block row is scaled
+ * by inv(M) (mkDenseBlockSystem.m:90-94).  Returns the number of singular diagonal blocks. */
+int orc_dense_block_system(int ne, int nfe, int npf, int ncu, int nf, const int *fel, const int *t2f,
+                           const int *elcon, const double *AE, const double *FE, int *f2f, double *K, double *F)
+{
+    const int nbf = 2 * nfe - 1, ncf = ncu * npf, ndf = npf * nfe, nh = ncu * ndf, nn = nbf - 1;
+    int nbad = 0;
+    double *M = malloc(sizeof(double) * ncf * ncf), *T = malloc(sizeof(double) * ncf * ncf);
+    int *j1 = malloc(sizeof(int) * npf), *j2 = malloc(sizeof(int) * npf), *j3 = malloc(sizeof(int) * npf);
+    memset(f2f, 0, sizeof(int) * (size_t)nbf * nf);
+    memset(K, 0, sizeof(double) * (size_t)ncf * ncf * nn * nf);
+    /* AE(c, n, a, c2, n2, a2, e) with AE [ncu, npf, nfe, ncu, npf, nfe, ne] */
+#define AEX(c, n, a, c2, n2, a2, e) AE[(c) + ncu * ((n) + npf * ((a) + nfe * ((size_t)(c2) + ncu * ((n2) + npf * ((a2) + (size_t)nfe * (e))))))]
+    for (int i = 0; i < nf; i++) {
+        const int e1 = fel[2 * i] - 1, e2 = fel[2 * i + 1] - 1;
+        const int ne2 = e2 >= 0 ? 2 : 1;
+        const int el[2] = {e1, e2};
+        int fi[2] = {-1, -1};
+        for (int q = 0; q < ne2; q++)
+            for (int a = 0; a < nfe; a++)
+                if (t2f[el[q] + ne * a] - 1 == i) { fi[q] = a; break; }
+        for (int n = 0; n < npf; n++) j1[n] = elcon[n + npf * fi[0] + (size_t)ndf * e1] - 1 - i * npf;
+        if (ne2 == 2)
+            for (int n = 0; n < npf; n++) j2[n] = elcon[n + npf * fi[1] + (size_t)ndf * e2] - 1 - i * npf;
+        f2f[nbf * i] = i + 1;
+        for (int c = 0; c < ncu; c++)
+            for (int n = 0; n < npf; n++) {
+                double fv = FE[c + ncu * (j1[n] + npf * fi[0]) + (size_t)nh * e1];
+                if (ne2 == 2) fv += FE[c + ncu * (j2[n] + npf * fi[1]) + (size_t)nh * e2];
+                F[c + ncu * n + (size_t)ncf * i] = fv;
+                for (int c2 = 0; c2 < ncu; c2++)
+                    for (int n2 = 0; n2 < npf; n2++) {
+                        double v = AEX(c, j1[n], fi[0], c2, j1[n2], fi[0], e1);
+                        if (ne2 == 2) v += AEX(c, j2[n], fi[1], c2, j2[n2], fi[1], e2);
+                        M[(c + ncu * n) + ncf * (c2 + ncu * n2)] = v;
+                    }
+            }
+        int k = 0;
+        for (int q = 0; q < ne2; q++) {
+            const int e = el[q], ia = fi[q];
+            const int *jq = q == 0 ? j1 : j2;
+            for (int is = 0; is < nfe; is++) {
+                if (is == ia) continue;
+                const int jf = t2f[e + ne * is] - 1;
+                f2f[(k + 1) + nbf * i] = jf + 1;
+                for (int n = 0; n < npf; n++) j3[n] = elcon[n + npf * is + (size_t)ndf * e] - 1 - jf * npf;
+                double *Kb = K + (size_t)ncf * ncf * (k + (size_t)nn * i);
+                for (int c = 0; c < ncu; c++)
+                    for (int n = 0; n < npf; n++)
+                        for (int c2 = 0; c2 < ncu; c2++)
+                            for (int n2 = 0; n2 < npf; n2++)
+                                Kb[(c + ncu * n) + ncf * (c2 + ncu * n2)] = AEX(c, jq[n], ia, c2, j3[n2], is, e);
+                k++;
+            }
+        }
+        /* Mi = inv(M); F(:,i) = Mi F(:,i); K(:,:,j,i) = Mi K(:,:,j,i) */
+        if (inv_inplace(ncf, M)) nbad++;
+        double *fcol = F + (size_t)ncf * i, *tmp = T;
+        for (int r = 0; r < ncf; r++) {
+            double s = 0.0;
+            for (int c = 0; c < ncf; c++) s += M[r + ncf * c] * fcol[c];
+            tmp[r] = s;
+        }
+        memcpy(fcol, tmp, sizeof(double) * ncf);
+        for (int q = 0; q < nn; q++) {
+            double *Kb = K + (size_t)ncf * ncf * (q + (size_t)nn * i);
+            mm(ncf, M, Kb, T);
+            memcpy(Kb, T, sizeof(double) * ncf * ncf);
+        }
+    }
+#undef AEX
+    free(M); free(T); free(j1); free(j2); free(j3);
+    return nbad;
+}
+
+/* kernel/gmres.m:40-44: y = x + K gather(x, f2f). */
+void orc_dense_matvec(int nb, int nf, int nbf, const double *K, const int *f2f, const double *x, double *y)
+{
+    const int nn = nbf - 1;
+    for (int i = 0; i < nf; i++)
+        for (int r = 0; r < nb; r++) {
+            double s = x[r + (size_t)nb * i];
+            for (int k = 0; k < nn; k++) {
+                const int j = f2f[(k + 1) + nbf * i];
+                if (j <= 0) continue;
+                const double *Kk = K + (size_t)nb * nb * (k + (size_t)nn * i);
+                for (int c = 0; c < nb; c++) s += Kk[r + nb * c] * x[c + (size_t)nb * (j - 1)];
+            }
+            y[r + (size_t)nb * i] = s;
+        }
+}
+
+/* kernel/gmres.m:1-111: unpreconditioned restarted GMRES on x + K gather(x) with classical
+ * Gram-Schmidt (gmres.m:80-81); the least-squares problem of gmres.m:90 is solved with Givens
+ * rotations (same minimiser and residual).  Iterations are counted as gmres.m counts them (the
+ * residual evaluation at each restart is one).  Returns iterations; *flag 0 converged /
+ * 1 maxit; rev[maxit] relative residuals (may be NULL). */
+int orc_gmres_dense(int nb, int nf, int nbf, const double *K, const int *f2f, const double *b, double *x,
+                    int restart, double tol, int maxit, int *flag, double *rev)
+{
+    const size_t N = (size_t)nb * nf;
+    double *t = malloc(sizeof(double) * N), *V = malloc(sizeof(double) * N * (restart + 1));
+    double *Hh = calloc((size_t)(restart + 1) * restart, sizeof(double));
+    double *cs = calloc(restart, sizeof(double)), *sn = calloc(restart, sizeof(double));
+    double *g = calloc(restart + 1, sizeof(double)), *y = calloc(restart, sizeof(double));
+    const double nrmb = nrm2(N, b);
+    int iter = 0;
+    *flag = 2;
+    if (!(nrmb > 0.0)) *flag = 0;
+    while (*flag == 2) {
+        orc_dense_matvec(nb, nf, nbf, K, f2f, x, t);
+        for (size_t q = 0; q < N; q++) V[q] = b[q] - t[q];
+        const double beta = nrm2(N, V);
+        double res = beta;
+        if (rev && iter < maxit) rev[iter] = res / nrmb;
+        iter++;
+        if (res / nrmb <= tol) { *flag = 0; break; }
+        if (iter >= maxit) { *flag = 1; break; }
+        for (size_t q = 0; q < N; q++) V[q] /= beta;
+        for (int q = 0; q <= restart; q++) g[q] = 0.0;
+        g[0] = beta;
+        int jdone = 0;
+        for (int j = 0; j < restart; j++) {
+            if (j > 0) {
+                if (res / nrmb <= tol) { *flag = 0; break; }
+                if (iter >= maxit) { *flag = 1; break; }
+            }
+            double *w = V + N * (j + 1), *hc = Hh + (size_t)(restart + 1) * j;
+            orc_dense_matvec(nb, nf, nbf, K, f2f, V + N * j, w);
+            for (int i = 0; i <= j; i++) {             /* h = V' w with the unmodified w */
+                const double *vi = V + N * i;
+                double h = 0.0;
+                for (size_t q = 0; q < N; q++) h += vi[q] * w[q];
+                hc[i] = h;
+            }
+            for (int i = 0; i <= j; i++) {
+                const double *vi = V + N * i;
+                for (size_t q = 0; q < N; q++) w[q] -= hc[i] * vi[q];
+            }
+            hc[j + 1] = nrm2(N, w);
+            const double sub = hc[j + 1];
+            if (sub != 0.0) for (size_t q = 0; q < N; q++) w[q] /= sub;
+            for (int i = 0; i < j; i++) {
+                const double a = hc[i], bb = hc[i + 1];
+                hc[i] = cs[i] * a + sn[i] * bb;
+                hc[i + 1] = -sn[i] * a + cs[i] * bb;
+            }
+            const double a = hc[j], bb = hc[j + 1], den = sqrt(a * a + bb * bb);
+            cs[j] = den != 0.0 ? a / den : 1.0; sn[j] = den != 0.0 ? bb / den : 0.0;
+            hc[j] = den; hc[j + 1] = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            res = fabs(g[j + 1]);
+            if (rev && iter < maxit) rev[iter] = res / nrmb;
+            iter++;
+            jdone = j + 1;
+            if (sub == 0.0) break;
+        }
+        for (int i = jdone - 1; i >= 0; i--) {
+            double s = g[i];
+            for (int l = i + 1; l < jdone; l++) s -= Hh[i + (size_t)(restart + 1) * l] * y[l];
+            y[i] = s / Hh[i + (size_t)(restart + 1) * i];
+        }
+        for (int i = 0; i < jdone; i++) for (size_t q = 0; q < N; q++) x[q] += V[N * i + q] * y[i];
+    }
+    free(t); free(V); free(Hh); free(cs); free(sn); free(g); free(y);
+    return iter;
 }

@@ -35,6 +35,12 @@ class HdgxBsr(ct.Structure):
                 ("sweep_plan", _dp), ("sweep_maxd", ct.c_int)]
 
 
+class HdgxElemBucket(ct.Structure):
+    _fields_ = [("master", _dp), ("app", _dp), ("ne", ct.c_int), ("dgnodes", _dp), ("bf", _dp), ("UDG", _dp),
+                ("UH", _dp), ("SH", _dp), ("AE", _dp), ("FE", _dp), ("DUDG", _dp), ("DUDG_DUH", _dp),
+                ("status", _dp), ("grid", ct.c_int)]
+
+
 class HdgxAssemblyMap(ct.Structure):
     _fields_ = [("blk_e", _dp), ("blk_ab", _dp), ("blk_row", _dp), ("face_e", _dp), ("face_a", _dp)]
 
@@ -99,6 +105,8 @@ def _declare(L):
     L.hdgx_gmres_bilu0_noalloc.argtypes = [B, v, v, v, v, i, d, i, p(i), p(i), p(d), v, v]
     L.hdgx_backsub.restype = i
     L.hdgx_backsub.argtypes = [i, i, i, i, i, v, v, v, v, v, v]
+    L.hdgx_elemental_buckets.restype = i
+    L.hdgx_elemental_buckets.argtypes = [i, v, i, v]
     L.hdgx_arraymul.restype = i
     L.hdgx_arraymul.argtypes = [i, i, i, i, i, i, v, v, v, v]
     L.hdgx_dense_block_system.restype = i

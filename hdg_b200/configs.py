@@ -8,6 +8,11 @@
   Fourier modes).
 * ``c4``: 3D steady Euler on tetrahedra, unit cube, 32^3 cubes x 6 = 196,608 elements,
   p = 2, Mach 0.4 + 1 % density perturbation of 6 Fourier modes.
+* ``c3``: 2D steady Euler, [0,10]^2, 181x181 squares x 2 = 65,522 elements, each of degree
+  p in {1, 2, 3, 4} drawn from the seed with proportions 0.2 / 0.4 / 0.3 / 0.1, Mach 0.6
+  freestream + vortex.  The reference defines no mixed-degree coupling, so every degree is a
+  bucket of elements evaluated as on the uniform-degree mesh of the same triangulation
+  (``MixedDegreeProblem``); the element work is what is measured.
 ``n`` overrides the number of squares / cubes per side (smaller parity cases).
 """
 from __future__ import annotations
@@ -66,5 +71,33 @@ def c4(seed=0, n=32, porder=2):
     return _finish("c4", master, mesh, app, u)
 
 
+@dataclass
+class MixedDegreeProblem:
+    name: str
+    degree: np.ndarray            # [ne] degree of every element
+    buckets: list                 # [(p, Problem on the uniform-degree mesh, element indices)]
+
+    @property
+    def ne(self):
+        return int(self.degree.shape[0])
+
+
+def c3(seed=0, n=181, degrees=(1, 2, 3, 4), proportions=(0.2, 0.4, 0.3, 0.1)):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ne = 2 * n * n
+    deg = rng.choice(np.asarray(degrees), size=ne, p=np.asarray(proportions))
+    buckets = []
+    for p in degrees:
+        idx = np.nonzero(deg == p)[0]
+        if idx.size == 0:
+            continue
+        mesh = mkmesh_square(n + 1, n + 1, p, 0, 10.0, 10.0)
+        master = mkmaster(2, p, 2 * p)
+        app = make_app(2, re=np.inf, minf=0.6, tau=2.0)
+        u = state_vortex(mesh.dgnodes, 1.4, 0.6, seed)
+        buckets.append((p, _finish(f"c3-p{p}", master, mesh, app, u), idx))
+    return MixedDegreeProblem("c3", deg, buckets)
+
+
 def by_name(name, **kw):
-    return {"c1": c1, "c2": c2, "c4": c4}[name](**kw)
+    return {"c1": c1, "c2": c2, "c3": c3, "c4": c4}[name](**kw)

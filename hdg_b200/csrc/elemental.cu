@@ -794,7 +794,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
 
 // ------------------------------------------------------------------ dispatch
 template <class D, bool VISC, bool MIXED>
-static int launch_t(const ElemParams &p, cudaStream_t st) {
+static int launch_t(const ElemParams &p, cudaStream_t st, int grid_req) {
     constexpr int NT = 256;
     using L = Plan<D, VISC, MIXED>;
     static_assert(L::TILE >= 1, "tile");
@@ -808,7 +808,7 @@ static int launch_t(const ElemParams &p, cudaStream_t st) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
     if (per_sm < 1) return -11;
-    int grid = nsm * per_sm;
+    int grid = grid_req > 0 ? grid_req : nsm * per_sm;     // default: one wave of resident CTAs
     if (grid > p.ne) grid = p.ne;
     if (grid < 1) return 0;
     kern<<<grid, NT, smem, st>>>(p);
@@ -817,14 +817,15 @@ static int launch_t(const ElemParams &p, cudaStream_t st) {
 }
 
 template <class D>
-static int launch_v(const ElemParams &p, bool visc, bool mixed, cudaStream_t st) {
-    if (mixed) return visc ? launch_t<D, true, true>(p, st) : launch_t<D, false, true>(p, st);
-    return visc ? launch_t<D, true, false>(p, st) : launch_t<D, false, false>(p, st);
+static int launch_v(const ElemParams &p, bool visc, bool mixed, cudaStream_t st, int grid) {
+    if (mixed) return visc ? launch_t<D, true, true>(p, st, grid) : launch_t<D, false, true>(p, st, grid);
+    return visc ? launch_t<D, true, false>(p, st, grid) : launch_t<D, false, false>(p, st, grid);
 }
 
 int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const double *dgnodes,
                      const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
-                     double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed) {
+                     double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed,
+                     int grid) {
     ElemParams p;
     p.shapvt = m->shapvt; p.shapvg = m->shapvg; p.shapmv = m->shapmv;
     p.shapft = m->shapft; p.shapfg = m->shapfg; p.shapmf = m->shapmf; p.perm = m->perm;
@@ -843,15 +844,15 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
     const int nd = m->nd, po = m->porder;
     if (nd == 2) {
         switch (po) {
-            case 1: return launch_v<Dims<2, 3, 2, 3, 2>>(p, visc, mixed, st);
-            case 2: return launch_v<Dims<2, 6, 3, 6, 3>>(p, visc, mixed, st);
-            case 3: return launch_v<Dims<2, 10, 4, 12, 4>>(p, visc, mixed, st);
-            case 4: return launch_v<Dims<2, 15, 5, 16, 5>>(p, visc, mixed, st);
+            case 1: return launch_v<Dims<2, 3, 2, 3, 2>>(p, visc, mixed, st, grid);
+            case 2: return launch_v<Dims<2, 6, 3, 6, 3>>(p, visc, mixed, st, grid);
+            case 3: return launch_v<Dims<2, 10, 4, 12, 4>>(p, visc, mixed, st, grid);
+            case 4: return launch_v<Dims<2, 15, 5, 16, 5>>(p, visc, mixed, st, grid);
         }
     } else if (nd == 3) {
         switch (po) {
-            case 1: return launch_v<Dims<3, 4, 3, 4, 3>>(p, visc, mixed, st);
-            case 2: return launch_v<Dims<3, 10, 6, 11, 6>>(p, visc, mixed, st);
+            case 1: return launch_v<Dims<3, 4, 3, 4, 3>>(p, visc, mixed, st, grid);
+            case 2: return launch_v<Dims<3, 10, 6, 11, 6>>(p, visc, mixed, st, grid);
         }
     }
     return -3;

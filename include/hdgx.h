@@ -105,6 +105,29 @@ int hdgx_schur_uq(int nd, int npv, int ncu, int ndf, int ne,
                   const double *Ru, const double *Rh, double *DUDG, double *DUDG_DUH,
                   double *AE, double *FE, int *status, hdgx_stream_t stream);
 
+/* One elemental evaluation over several buckets of elements (e.g. one per polynomial degree
+ * of a mixed-degree mesh), each with its own master, app and arrays (layouts as
+ * hdgx_elemental).  The buckets' kernels run concurrently on side streams forked from and
+ * joined back into `stream`, so the whole call is one node sequence of a CUDA graph when the
+ * caller captures it (make one uncaptured call first: it creates the side streams and sets
+ * the kernels' shared-memory limits).  grid = CTAs of the bucket's launch (0: one wave of
+ * resident CTAs on the whole GPU).  mixed != 0 selects the mixed-precision kernel.  No
+ * counterpart in the reference, which has no mixed-degree meshes (kernel/hdg_elemental.m is
+ * called per uniform mesh). */
+typedef struct {
+    const hdgx_master *master;
+    const hdgx_app *app;
+    int ne;
+    const double *dgnodes;
+    const int *bf;
+    const double *UDG, *UH, *SH;
+    double *AE, *FE, *DUDG, *DUDG_DUH;
+    int *status;
+    int grid;
+} hdgx_elem_bucket;
+
+int hdgx_elemental_buckets(int nb, const hdgx_elem_bucket *buckets, int mixed, hdgx_stream_t stream);
+
 /* Batched u-only Schur complement (kernel/schur_u.c): BD[npv,ncu,npv,nc,ne] (only the
  * first ncu component columns are read), F, GK[ncu,ndf,npv,nc,ne], H, Ru, Rh ->
  * DUDG[npv,nc,ne], DUDG_DUH[npv,nc,ncu,ndf,ne] (components >= ncu set to 0), AE, FE. */

@@ -474,7 +474,49 @@ def newton_step(P, torch, args):
         del s
         torch.cuda.empty_cache()
     res["note"] = "one Newton iteration incl. initial assembly, BILU(0)-GMRES(20) to 1e-10, back-substitution, line-search re-assembly"
+    res["breakdown"] = newton_breakdown(P, torch)
     return res
+
+
+def newton_breakdown(P, torch):
+    """CUDA-event times of the operations of one Newton linear solve (FP64, MDF order)."""
+    from hdg_b200.elemental import DArray
+    from hdg_b200.solve import HDGSolver
+    s = HDGSolver(P.master, P.mesh, P.app)
+    U = DArray.from_numpy(P.UDG); H = DArray.from_numpy(P.UH); S = DArray.from_numpy(P.SH)
+
+    def timed(fn, reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    out = {}
+    s.assemble(U, H, S)
+    out["assemble_ms"] = timed(lambda: s.assemble(U, H, S), 3)
+    t0 = time.perf_counter()
+    s.ts.bilu0(s.Hg, s.Mg)
+    torch.cuda.synchronize()
+    out["first_factor_with_mdf_order_ms"] = 1e3 * (time.perf_counter() - t0)
+    out["bilu0_factor_ms"] = timed(lambda: s.ts.bilu0(s.Hg, s.Mg), 2)
+    x, w = s.ts.empty_vec(), s.ts.empty_vec()
+    out["bilu0_apply_ms"] = timed(lambda: s.ts.bilu0_apply(s.Mg, s.Rg, x, w), 10)
+    out["matvec_ms"] = timed(lambda: s.ts.matvec(s.Hg, s.Rg, x), 10)
+    s.DUH.t.zero_()
+    t0 = time.perf_counter()
+    gi, _, _, _ = s.ts.gmres(s.Hg, s.Mg, s.Rg, s.DUH, 20, 1e-10, 1000, s.ws)
+    torch.cuda.synchronize()
+    out["gmres_ms"] = 1e3 * (time.perf_counter() - t0)
+    out["gmres_iterations"] = gi
+    out["backsub_ms"] = timed(lambda: s.backsub(), 5)
+    out["levels"] = int(s.ts.ord.ncolors)
+    del s
+    torch.cuda.empty_cache()
+    return out
 
 
 if __name__ == "__main__":

@@ -41,6 +41,25 @@ class HdgxElemBucket(ct.Structure):
                 ("status", _dp), ("grid", ct.c_int)]
 
 
+HDGX_SOLVE_MAXIT = 16
+
+
+class HdgxMesh(ct.Structure):
+    _fields_ = [("ne", ct.c_int), ("nf", ct.c_int), ("dgnodes", _dp), ("bf", _dp), ("elcon", _dp), ("t2f", _dp),
+                ("rowpts", _dp), ("colind", _dp)]
+
+
+class HdgxSolveOpts(ct.Structure):
+    _fields_ = [("ordering", ct.c_int), ("mixed", ct.c_int), ("restart", ct.c_int), ("maxiter", ct.c_int),
+                ("tol", ct.c_double), ("gmres_tol", ct.c_double), ("gmres_maxit", ct.c_int)]
+
+
+class HdgxSolveReport(ct.Structure):
+    _fields_ = [("iterations", ct.c_int), ("converged", ct.c_int), ("ncolors", ct.c_int),
+                ("residuals", ct.c_double * (HDGX_SOLVE_MAXIT + 1)), ("alphas", ct.c_double * HDGX_SOLVE_MAXIT),
+                ("gmres_iters", ct.c_int * HDGX_SOLVE_MAXIT), ("gmres_relres", ct.c_double * HDGX_SOLVE_MAXIT)]
+
+
 class HdgxAssemblyMap(ct.Structure):
     _fields_ = [("blk_e", _dp), ("blk_ab", _dp), ("blk_row", _dp), ("face_e", _dp), ("face_a", _dp)]
 
@@ -105,6 +124,8 @@ def _declare(L):
     L.hdgx_gmres_bilu0_noalloc.argtypes = [B, v, v, v, v, i, d, i, p(i), p(i), p(d), v, v]
     L.hdgx_backsub.restype = i
     L.hdgx_backsub.argtypes = [i, i, i, i, i, v, v, v, v, v, v]
+    L.hdgx_solve.restype = i
+    L.hdgx_solve.argtypes = [p(HdgxMaster), p(HdgxApp), p(HdgxMesh), v, v, v, p(HdgxSolveOpts), p(HdgxSolveReport), v]
     L.hdgx_elemental_buckets.restype = i
     L.hdgx_elemental_buckets.argtypes = [i, v, i, v]
     L.hdgx_arraymul.restype = i

@@ -293,3 +293,37 @@ def hdg_solve(master, mesh, app, UDG, UH, SH=None, tol=1e-10, maxiter=16, gmres_
     dS = DArray.from_numpy(np.zeros_like(UDG) if SH is None else SH)
     rep = s.solve(dU, dH, dS, tol=tol, maxiter=maxiter, gmres_tol=gmres_tol)
     return dU.numpy(), dH.numpy(), rep
+
+
+def hdgx_solve(master, mesh, app, UDG, UH, SH=None, tol=1e-10, maxiter=16, gmres_tol=1e-10, restart=20,
+               ordering="mdf", mixed=False, gmres_maxit=1000, stream=None):
+    """kernel/hdg_solve.m as ONE native call (``hdgx_solve`` of the C ABI): the Newton loop,
+    the elimination order and the assembly map are built inside the library.  Returns
+    (UDG, UH, report dict) as host arrays; the inputs are not modified."""
+    from ._lib import HDGX_SOLVE_MAXIT, HdgxMesh, HdgxSolveOpts, HdgxSolveReport
+    _require_cuda()
+    if maxiter > HDGX_SOLVE_MAXIT:
+        raise ValueError(f"maxiter <= {HDGX_SOLVE_MAXIT}")
+    dm = DeviceMaster(master)
+    appc = app_struct(app)
+    dg = DArray.from_numpy(mesh.dgnodes)
+    bf = DArray.from_numpy(mesh.bf, dtype=torch.int32)
+    el = DArray.from_numpy(mesh.elcon, dtype=torch.int32)
+    t2f = np.asfortranarray(mesh.t2f, dtype=np.int32)
+    rp = np.ascontiguousarray(mesh.cbsr_rowpts, dtype=np.int64)
+    ci = np.ascontiguousarray(mesh.cbsr_colind, dtype=np.int32)
+    cm = HdgxMesh(mesh.ne, mesh.nf, dg.ptr, bf.ptr, el.ptr, t2f.ctypes.data, rp.ctypes.data, ci.ctypes.data)
+    opts = HdgxSolveOpts({"mdf": 0, "multicolor": 1}[ordering], int(mixed), int(restart), int(maxiter), float(tol),
+                         float(gmres_tol), int(gmres_maxit))
+    dU = DArray.from_numpy(UDG)
+    dH = DArray.from_numpy(UH)
+    dS = DArray.from_numpy(np.zeros_like(UDG) if SH is None else SH)
+    rep = HdgxSolveReport()
+    rc = lib().hdgx_solve(ct.byref(dm.c), ct.byref(appc), ct.byref(cm), dU.ptr, dH.ptr, dS.ptr, ct.byref(opts),
+                          ct.byref(rep), _stream_ptr(stream))
+    check(rc, "hdgx_solve")
+    n = rep.iterations
+    report = dict(iterations=n, converged=bool(rep.converged), levels=rep.ncolors,
+                  residuals=list(rep.residuals[:n + 1]), alphas=list(rep.alphas[:n]),
+                  gmres_iters=list(rep.gmres_iters[:n]), gmres_relres=list(rep.gmres_relres[:n]))
+    return dU.numpy(), dH.numpy(), report

@@ -22,6 +22,7 @@
  *   hdgx_gmres_bilu0      kernel/gmres_bilu0.m:1     [x,flags,iter,rev] = gmres_bilu0(mesh,M,A,b,x,restart,tol,maxit)
  *   hdgx_backsub          kernel/hdg_solve.m:119-121 DUDGT = DUDG + mapContractK(DUDG_DUH, DUH(elcon))
  *   hdgx_gather_uh        kernel/hdg_assemble.m:34   uh = reshape(UH(:,elcon),[ncu npf*nfe ne])
+ *   hdgx_solve            kernel/hdg_solve.m:1       [UDG,UH] = hdg_solve(master,mesh,app,UDG,UH,SH)
  *   hdgx_arraymul         kernel/arraymul.c:11       C = arraymul(A,B)
  *   hdgx_dense_block_system kernel/mkDenseBlockSystem.m:9  [K,F] = mkDenseBlockSystem(AE,FE,f,t2f,elcon)
  *   hdgx_dense_matvec     kernel/gmres.m:40-44       d = x + arraymul(K, gather(x, f2f))
@@ -234,6 +235,48 @@ int hdgx_gmres_bilu0_noalloc(const hdgx_bsr *A, const double *Hg, const double *
  * DUH[ncu, nsiz]. */
 int hdgx_backsub(int npv, int nc, int ncu, int ndf, int ne, const int *elcon, const double *DUDG,
                  const double *DUDG_DUH, const double *DUH, double *DUDGT, hdgx_stream_t stream);
+
+/* ---------------------------------------------------------------- Newton solve */
+
+#define HDGX_SOLVE_MAXIT 16   /* hdg_solve.m:108: at most 16 Newton steps */
+
+/* The mesh of hdgx_solve: per-element arrays on the DEVICE, connectivity on the HOST. */
+typedef struct {
+    int ne, nf;
+    const double *dgnodes;     /* device [npv, nd, ne] */
+    const int *bf;             /* device [nfe, ne] (bf < 0: boundary index -bf) */
+    const int *elcon;          /* device [npf*nfe, ne], 1-based trace nodes */
+    const int *t2f;            /* HOST [ne, nfe] column-major, 1-based faces */
+    const long long *rowpts;   /* HOST [nf+1] block-CSR offsets (mesh.cbsr_rowpts) */
+    const int *colind;         /* HOST [nnzb] 1-based, diagonal first (mesh.cbsr_colind) */
+} hdgx_mesh;
+
+typedef struct {
+    int ordering;              /* 0: minimum-discarded-fill (computeMDFordering.m), 1: greedy multicolour */
+    int mixed;                 /* 1: mixed-precision elemental kernel */
+    int restart;               /* GMRES restart (20) */
+    int maxiter;               /* Newton steps (<= HDGX_SOLVE_MAXIT) */
+    double tol;                /* Newton stop: |F| / |F0| <= tol (hdg_solve.m:107 uses 1e-9) */
+    double gmres_tol;          /* BILU(0)-GMRES relative tolerance */
+    int gmres_maxit;
+} hdgx_solve_opts;
+
+typedef struct {
+    int iterations, converged, ncolors;
+    double residuals[HDGX_SOLVE_MAXIT + 1];   /* |F| before the first and after every Newton step */
+    double alphas[HDGX_SOLVE_MAXIT];          /* line-search step lengths */
+    int gmres_iters[HDGX_SOLVE_MAXIT];
+    double gmres_relres[HDGX_SOLVE_MAXIT];
+} hdgx_solve_report;
+
+/* Newton solve of kernel/hdg_solve.m:84-176 on the device: assembly (hdg_assemble.m), BILU(0)-
+ * GMRES with x0 = 0 in place of K\F, back-substitution (hdg_solve.m:119-121) and the halving
+ * line search (hdg_solve.m:144-163), until |F| / |F0| <= tol or maxiter steps.  UDG [npv,nc,ne]
+ * and UH [ncu, nf*npf] (device) are updated in place; SH [npv,nc,ne] (device) is the source.
+ * Workspace comes from the stream-ordered allocator and is released before returning; the
+ * call synchronises the stream (it reads residual norms on the host). */
+int hdgx_solve(const hdgx_master *master, const hdgx_app *app, const hdgx_mesh *mesh, double *UDG, double *UH,
+               const double *SH, const hdgx_solve_opts *opts, hdgx_solve_report *report, hdgx_stream_t stream);
 
 /* ------------------------------------------------- dense face-block path (app.denseblock = 1) */
 

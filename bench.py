@@ -445,11 +445,20 @@ def serve_mix(torch, count=16, slots=8, ordering="mdf"):
     s_conc = Server(slots=slots, ordering=ordering).serve(conc)
     same = all(a.UDG is not None and b.UDG is not None and np.array_equal(a.UDG, b.UDG)
                and np.array_equal(a.UH, b.UH) for a, b in zip(seq, conc))
+    # capacity: 4x as many requests, all waiting at t = 0 (the arrival rate no longer caps the
+    # rate, and no single large request sets the makespan)
+    seq2 = request_mix(12, 4 * count, **kw)
+    c_seq = Server(slots=1, ordering=ordering).serve_sequential(seq2, realtime=False)
+    conc2 = request_mix(12, 4 * count, **kw)
+    c_conc = Server(slots=slots, ordering=ordering).serve(conc2, realtime=False)
     torch.cuda.empty_cache()
     return {"requests": count, "slots": slots, "ordering": ordering, "newton_tol": 1e-10,
             "mix": "2D n x n x 2, n 8-20, p 1-4, M 0.3-0.8, half Euler / half NS Re 200-2000, Poisson 20/s (seed 11)",
             "concurrent": s_conc, "sequential": s_seq, "identical_alone_vs_mix": bool(same),
-            "speedup_solves_per_s": s_conc["solves_per_s"] / s_seq["solves_per_s"]}
+            "speedup_solves_per_s": s_conc["solves_per_s"] / s_seq["solves_per_s"],
+            "capacity": {"note": f"{4 * count} requests of the same distribution (seed 12), all queued at t = 0",
+                         "concurrent": c_conc, "sequential": c_seq,
+                         "speedup_solves_per_s": c_conc["solves_per_s"] / c_seq["solves_per_s"]}}
 
 
 def newton_step(P, torch, args):

@@ -8,10 +8,12 @@
 // search of hdg_solve.m:144-163.  The host-side set-up it needs (element -> block assembly map,
 // elimination order, level schedule, sweep records) is built here from the mesh's host
 // connectivity.  Every device buffer comes from the stream-ordered allocator and is released
-// before returning.
+// before returning, into a private pool that keeps up to 8 GiB of freed memory for the next
+// solve.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <algorithm>
+#include <mutex>
 #include <vector>
 #include "hdgx_common.cuh"
 
@@ -155,17 +157,44 @@ void build_levels(int nf, const long long *rowpts, const int *colind, const std:
     }
 }
 
+// A private stream-ordered memory pool per device.  Freed blocks stay in the pool up to
+// kKeepBytes across synchronisations (the default pool returns everything to the driver at
+// every synchronisation, and remapping it on the next solve costs more than a small solve).
+constexpr int kMaxDev = 64;
+constexpr unsigned long long kKeepBytes = 8ull << 30;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxDev] = {};
+
+cudaMemPool_t solve_pool() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return nullptr;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+        unsigned long long keep = kKeepBytes;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        g_pool[dev] = p;
+    }
+    return g_pool[dev];
+}
+
 // device buffers from the stream-ordered allocator, released together
 struct DevPool {
     cudaStream_t st;
+    cudaMemPool_t pool;
     std::vector<void *> ptrs;
     bool failed = false;
-    explicit DevPool(cudaStream_t s) : st(s) {}
+    explicit DevPool(cudaStream_t s) : st(s), pool(solve_pool()) { if (!pool) failed = true; }
     template <class T>
     T *get(size_t n) {
         void *p = nullptr;
         if (n == 0) n = 1;
-        if (cudaMallocAsync(&p, sizeof(T) * n, st) != cudaSuccess) { failed = true; return nullptr; }
+        if (!pool || cudaMallocFromPoolAsync(&p, sizeof(T) * n, pool, st) != cudaSuccess) { failed = true; return nullptr; }
         ptrs.push_back(p);
         return (T *)p;
     }

@@ -92,10 +92,22 @@ def request_mix(seed, count, nmin=8, nmax=24, pmin=1, pmax=4, rate=20.0):
     return reqs
 
 
-def _solve_one(req, ordering, mixed, restart):
+def _solve_one(req, ordering, mixed, restart, engine="native"):
+    """One request on the current CUDA stream.  engine "native": one hdgx_solve call (the
+    Newton loop and its host-side set-up in the library, which runs without the Python
+    interpreter lock, so concurrent requests also overlap on the host); "python": the
+    HDGSolver composition of the same kernels."""
+    P = req.problem
+    if engine == "native":
+        from .solve import hdgx_solve
+        U, H, rep = hdgx_solve(P.master, P.mesh, P.app, P.UDG, P.UH, P.SH, tol=req.tol, maxiter=req.maxiter,
+                               restart=restart, ordering=ordering, mixed=mixed)
+        req.UDG, req.UH = U, H
+        req.converged, req.iterations = rep["converged"], rep["iterations"]
+        req.residuals, req.gmres_iters = list(rep["residuals"]), list(rep["gmres_iters"])
+        return
     from .elemental import DArray
     from .solve import HDGSolver
-    P = req.problem
     s = HDGSolver(P.master, P.mesh, P.app, ordering=ordering, restart=restart, mixed=mixed)
     U = DArray.from_numpy(P.UDG)
     H = DArray.from_numpy(P.UH)
@@ -117,12 +129,12 @@ def latency_stats(reqs, t0):
 
 
 class Server:
-    def __init__(self, slots=8, memory_budget=None, ordering="multicolor", mixed=False, restart=20):
+    def __init__(self, slots=8, memory_budget=None, ordering="multicolor", mixed=False, restart=20, engine="native"):
         if memory_budget is None:
             free, _ = torch.cuda.mem_get_info()
             memory_budget = int(0.8 * free)
         self.slots, self.budget = slots, memory_budget
-        self.ordering, self.mixed, self.restart = ordering, mixed, restart
+        self.ordering, self.mixed, self.restart, self.engine = ordering, mixed, restart, engine
 
     def serve(self, reqs, realtime=True):
         """Run the requests with continuous admission; returns latency statistics."""
@@ -142,7 +154,7 @@ class Server:
             torch.cuda.set_device(dev)
             try:
                 with torch.cuda.stream(streams[sid]):
-                    _solve_one(req, self.ordering, self.mixed, self.restart)
+                    _solve_one(req, self.ordering, self.mixed, self.restart, self.engine)
                 streams[sid].synchronize()
             except Exception as exc:        # a failed request is reported, not fatal
                 req.error = repr(exc)
@@ -190,7 +202,7 @@ class Server:
                 req.arrival = 0.0
             req.admitted = time.perf_counter() - t0
             try:
-                _solve_one(req, self.ordering, self.mixed, self.restart)
+                _solve_one(req, self.ordering, self.mixed, self.restart, self.engine)
             except Exception as exc:
                 req.error = repr(exc)
             torch.cuda.synchronize()

@@ -273,8 +273,9 @@ typedef struct {
  * GMRES with x0 = 0 in place of K\F, back-substitution (hdg_solve.m:119-121) and the halving
  * line search (hdg_solve.m:144-163), until |F| / |F0| <= tol or maxiter steps.  UDG [npv,nc,ne]
  * and UH [ncu, nf*npf] (device) are updated in place; SH [npv,nc,ne] (device) is the source.
- * Workspace comes from the stream-ordered allocator and is released before returning; the
- * call synchronises the stream (it reads residual norms on the host). */
+ * Workspace comes from a private stream-ordered memory pool of the library (one per device) and
+ * is released into it before returning; the pool keeps up to 8 GiB of freed memory for later
+ * calls.  The call synchronises the stream (it reads residual norms on the host). */
 int hdgx_solve(const hdgx_master *master, const hdgx_app *app, const hdgx_mesh *mesh, double *UDG, double *UH,
                const double *SH, const hdgx_solve_opts *opts, hdgx_solve_report *report, hdgx_stream_t stream);
 

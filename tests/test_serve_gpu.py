@@ -13,15 +13,15 @@ def _mix(seed=3, count=5):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("ordering", ["multicolor", "mdf"])
-def test_results_identical_alone_and_in_mix(ordering):
+@pytest.mark.parametrize("ordering,engine", [("multicolor", "native"), ("mdf", "native"), ("mdf", "python")])
+def test_results_identical_alone_and_in_mix(ordering, engine):
     # the mix holds several block sizes (p = 1..3), so kernels shared by the requests are
     # launched concurrently with different shared-memory sizes
     from hdg_b200.serve import Server
     alone = _mix()
-    Server(slots=1, ordering=ordering).serve_sequential(alone, realtime=False)
+    Server(slots=1, ordering=ordering, engine=engine).serve_sequential(alone, realtime=False)
     mixed = _mix()
-    stats = Server(slots=4, ordering=ordering).serve(mixed, realtime=False)
+    stats = Server(slots=4, ordering=ordering, engine=engine).serve(mixed, realtime=False)
     assert stats["converged"] == len(mixed)
     for a, b in zip(alone, mixed):
         assert a.error == "" and b.error == ""

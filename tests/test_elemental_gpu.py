@@ -75,3 +75,27 @@ def test_elemental_repeatable_and_batch_independent(oracle):
         f, g, h = getattr(full, k).numpy(), getattr(again, k).numpy(), getattr(part, k).numpy()
         assert np.array_equal(f, g)
         assert np.array_equal(f[..., sl], h)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw", [("c2", dict(n=4, porder=3)), ("c1", dict(n=4, porder=2))])
+def test_curved_elements_match_oracle(oracle, name, kw):
+    """Elements with a non-constant jacobian (nodes moved off the straight-sided positions)
+    take the general path of the kernel (elimination of the mass matrix per element)."""
+    from hdg_b200.elemental import hdg_elemental
+    P = configs.by_name(name, **kw)
+    m, a = P.master, P.app
+    dg = np.array(P.mesh.dgnodes, copy=True)
+    x, y = dg[:, 0, :], dg[:, 1, :]
+    L = x.max() - x.min()
+    dg[:, 0, :] = x + 0.01 * L * np.sin(2 * np.pi * y / L) * np.sin(np.pi * x / L)
+    dg[:, 1, :] = y + 0.01 * L * np.sin(2 * np.pi * x / L) * np.sin(np.pi * y / L)
+    ref = oracle.hdg_elemental(m, a, dg, P.mesh.bf, P.UDG, P.uh_elem(), P.SH)
+    assert ref["nbad"] == 0
+    out = hdg_elemental(m, a, dg, P.mesh.bf, P.UDG, P.uh_elem(), P.SH)
+    assert int(out.status.numpy().max()) == 0
+    for k in ("AE", "FE", "DUDG_DUH"):
+        err = relerr(getattr(out, k).numpy(), ref[k])
+        assert err < TOL, f"curved {name} {k} relerr {err:.3e}"
+    err = relerr(out.DUDG.numpy(), ref["DUDG"])
+    assert err < max(TOL, 10.0 * ulp_sensitivity(oracle, P)), f"curved {name} DUDG relerr {err:.3e}"

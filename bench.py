@@ -1,9 +1,9 @@
 #!/usr/bin/env python
-"""Benchmark of the HDG elemental step on B200 (see the module-level CONFIG note below).
+"""Benchmark of the HDG elemental step on B200.
 
 One step = one fused FP64 elemental evaluation (volume + face integrals + local (u,q) Schur
 elimination -> AE, FE, DUDG, DUDG_DUH) over every element of the workload, inputs resident
-in HBM.  Workload (the north-star's FP64-vs-mixed NS configuration): 2D steady compressible
+in HBM.  Workload (the FP64-vs-mixed Navier-Stokes configuration): 2D steady compressible
 Navier-Stokes, Re 1000, Pr 0.72, Mach 0.3, [0,1]^2 as 128x128 squares x 2 triangles =
 32,768 elements, p = 3 (local (u,q) block 120x120, trace block 48x48), seeded synthetic state.
 

@@ -1,7 +1,7 @@
 """Mixed-precision elemental kernel (hdgx_elemental_mixed).
 
 Residual quantities stay FP64: FE (the condensed residual) and DUDG must match the FP64
-oracle to 1e-10 relative (the north-star accuracy bound; DUDG with the same ulp-sensitivity
+oracle to 1e-10 relative (the accuracy bound of the mixed form; DUDG with the same ulp-sensitivity
 allowance as the FP64 test).  AE and DUDG_DUH are Jacobians computed in FP32 and must match
 to 1e-4 relative.  The Newton solve with the mixed kernel must reach |F|/|F0| <= 1e-10 and
 agree with the FP64 solve's solution to 1e-9."""

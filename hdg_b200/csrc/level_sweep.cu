@@ -59,6 +59,9 @@ struct RowPrefetch {
                     const double *B = Mg + (size_t)BS * BS * k[d] + r;
 #pragma unroll
                     for (int c = 0; c < BS; c++) lv[d * BS + c] = __ldg(B + BS * c);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < BS; c++) lv[d * BS + c] = 0.0;     // padded slot: contributes 0
                 }
             }
             if constexpr (DIAG) {
@@ -71,6 +74,23 @@ struct RowPrefetch {
 
     // acc - sum_d B_d[r, :] in_{j_d}
     __device__ __forceinline__ double reduce(double acc, const double *__restrict__ Mg, const double *in, int r) const {
+        if constexpr (PL) {
+            // every neighbour's values are loaded before the first multiply-add, so their L2
+            // round trips overlap; padded slots (k < 0) contribute exact zeros
+            double ov[MAXD][BS];
+#pragma unroll
+            for (int d = 0; d < MAXD; d++) {
+                const bool live = k[d] >= 0;
+                const double *oj = in + (size_t)BS * (live ? j[d] : 0);
+#pragma unroll
+                for (int c = 0; c < BS; c++) ov[d][c] = live ? __ldcg(oj + c) : 0.0;
+            }
+#pragma unroll
+            for (int d = 0; d < MAXD; d++)
+#pragma unroll
+                for (int c = 0; c < BS; c++) acc -= lv[d * BS + c] * ov[d][c];
+            return acc;
+        }
 #pragma unroll
         for (int d = 0; d < MAXD; d++) {
             if (k[d] < 0) break;

@@ -41,6 +41,22 @@ WORKLOADS = {
 }
 
 
+def max_over_ranks(ms, ws, device):
+    """The slowest rank's time (every rank takes part; world size 1: unchanged)."""
+    if ws <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, ws, steps, total_ms):
+    """Whole-job throughput: the units of all ranks over the slowest rank's time."""
+    return ws * units_per_rank * steps / (total_ms * 1e-3)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -284,12 +300,9 @@ def main():
     clocks = sampler.stop()
     total_ms = t0.elapsed_time(t1)
     kern_ms = [s.elapsed_time(e) for s, e in ev]
-    if ws > 1:
-        tt = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = max_over_ranks(total_ms, ws, "cuda")
     ms_per_step = total_ms / args.steps
-    value = ws * ne * args.steps / (total_ms * 1e-3)
+    value = job_rate(ne, ws, args.steps, total_ms)
     # the other precision, same protocol (no clock sampling)
     other = step_fp64 if use_mixed else step_mixed
     o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -184,7 +184,8 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NT)
             if (pf.i >= 0) tsh[m * BS + r] = pf.reduce(__ldcg(y + (size_t)BS * pf.i + r), Mg, v, r);
             __syncthreads();
             if (pf.i >= 0) v[(size_t)BS * pf.i + r] = pf.diag(Mg, tsh + m * BS, r);
-            __syncthreads();
+            if (nr > CS * RPP) __syncthreads();      // tsh is rewritten by the next pass (else the
+                                                     // cluster barrier below orders its reuse)
             for (int base = CS * RPP; base < nr; base += CS * RPP) {    // trip count is uniform in the CTA
                 const int s = base + rank + CS * m;
                 const bool act = m < RPP && s < nr;

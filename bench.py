@@ -226,7 +226,7 @@ def main():
     ap.add_argument("--no-newton", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-buckets", action="store_true")
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"])
     ap.add_argument("--n", type=int, default=None, help="squares/cubes per side (smaller profiling cases)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.config])

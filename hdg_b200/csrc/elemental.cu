@@ -47,69 +47,80 @@ struct Dims {
 };
 
 // Shared-memory plan (in doubles).  "P" = persistent through the element, "X" = the
-// assembly-phase scratch, reused by the DUDG_DUH / AE column tiles at the end.
+// assembly-phase scratch, reused by the DUDG_DUH / AE column tiles at the end.  The scratch
+// is ordered so that everything the SD build does not read comes first (dead once the
+// right-hand sides and Rh are built); when it is large enough SD is built on top of it
+// (SD_ALIAS), and in the mixed form the FP32 inverse of SD follows it (the rest of the scratch
+// is dead during the solve).  The geometry tables shapmv / shapmf are read from global
+// memory (L1) instead: they are used once per element.  Less shared memory per element means
+// more elements resident per SM (the kernel is latency-bound).
 template <class D, bool VISC, bool MIXED = false>
 struct Plan {
     // master tables (loaded once per CTA)
     static constexpr int t_vt = 0;
     static constexpr int t_vg = t_vt + D::NGV * D::NPV * (D::ND + 1);
-    static constexpr int t_mv = t_vg + D::NPV * D::NGV * (D::ND + 1);
-    static constexpr int t_ft = t_mv + D::NGV * D::NPV * (D::ND + 1);
+    static constexpr int t_ft = t_vg + D::NPV * D::NGV * (D::ND + 1);
     static constexpr int t_fg = t_ft + D::NGF * D::NPF;
-    static constexpr int t_mf = t_fg + D::NPF * D::NGF;
+    // assembly scratch, first group: not read by the SD build
+    static constexpr int x_start = t_fg + D::NPF * D::NGF;
+    static constexpr int x_Xx = x_start;                          // [NGV, ND, ND]
+    static constexpr int x_jac = x_Xx + D::NGV * D::ND * D::ND;
+    static constexpr int x_nl = x_jac + D::NGV;                   // [NGT, ND]
+    static constexpr int x_jf = x_nl + D::NGT * D::ND;
+    static constexpr int x_ug = x_jf + D::NGT;                    // [NGV, NC]
+    static constexpr int x_fu = x_ug + D::NGV * D::NC;            // [NGT, NC]
+    static constexpr int x_fuh = x_fu + D::NGT * D::NC;           // [NGT, NCU]
+    static constexpr int x_wrk = x_fuh + D::NGT * D::NCU;         // [NGV, ND, NCU]
+    static constexpr int x_FH = x_wrk + D::NGV * D::ND * D::NCU;  // [NGT, NCU] jac*fhat
+    static constexpr int x_BH = x_FH + D::NGT * D::NCU;           // [NGT, NCU] jac*(fbou or fhat)
+    static constexpr int x_FHh = x_BH + D::NGT * D::NCU;          // [NGT, NCU, NCU] jac*dfhat/duh
+    static constexpr int x_Ze = x_FHh + D::NGT * D::NCU * D::NCU; // [NGV, NDF, ND]
+    static constexpr int x_Zr = x_Ze + (VISC ? D::NGV * D::NDF * D::ND : 0);   // [NGV, NCU, ND]
+    static constexpr int x_ZFe = x_Zr + (VISC ? D::NGV * D::NCU * D::ND : 0);  // [NGT, NDF, ND]
+    static constexpr int x_ZFr = x_ZFe + (VISC ? D::NGT * D::NDF * D::ND : 0); // [NGT, NCU, ND]
+    static constexpr int p_M = x_ZFr + (VISC ? D::NGT * D::NCU * D::ND : 0);   // mass matrix (dead after inv(M))
+    static constexpr int x_dead_end = p_M + D::NPV * D::NPV;
+    // second group: read by the SD build
+    static constexpr int x_wrl = x_dead_end;                      // [NGV, ND, NCU, NC]
+    static constexpr int x_FHu = x_wrl + D::NGV * D::ND * D::NCU * D::NC;  // [NGT, NCU, NC] jac*dfhat/dudg
+    static constexpr int x_Zc = x_FHu + D::NGT * D::NCU * D::NC;  // [NGV, NPV, ND]
+    static constexpr int x_ZFc = x_Zc + (VISC ? D::NGV * D::NPV * D::ND : 0);  // [NGT, NPV, ND]
+    static constexpr int x_end = x_ZFc + (VISC ? D::NGT * D::NPV * D::ND : 0);
+    static constexpr int x_size = x_end - x_start;
+    static constexpr bool SD_ALIAS = D::NU * D::NU <= x_dead_end - x_start;
+    static constexpr bool INV_ALIAS = MIXED && (SD_ALIAS ? 2 : 1) * D::NU * D::NU <= x_size;
     // persistent per element
-    static constexpr int p_dg = t_mf + D::NGF * D::NPF * D::ND;
+    static constexpr int p_dg = x_end;
     static constexpr int p_udg = p_dg + D::NPV * D::ND;
     static constexpr int p_uh = p_udg + D::NPV * D::NC;
-    static constexpr int p_SD = p_uh + D::NCU * D::NDF;
-    static constexpr int p_R = p_SD + D::NU * D::NU;              // [NU, 1+NH]
+    static constexpr int p_R = p_uh + D::NCU * D::NDF;            // [NU, 1+NH]
     static constexpr int p_MiC = p_R + D::NU * (1 + D::NH);       // [NPV, NPV*ND] | MiE | MiRq contiguous
     static constexpr int p_MiE = p_MiC + D::NPV * D::NPV * D::ND;
     static constexpr int p_MiRq = p_MiE + D::NPV * D::NDF * D::ND;
     static constexpr int p_Gp = p_MiRq + D::NPV * D::NCU * D::ND; // [NGT, NCU, NC] jac * dRh-flux/dudg
     static constexpr int p_Hp = p_Gp + D::NGT * D::NCU * D::NC;   // [NGT, NCU, NCU] jac * dRh-flux/duh
     static constexpr int p_Rh = p_Hp + D::NGT * D::NCU * D::NCU;
-    static constexpr int p_M = p_Rh + D::NH;
-    static constexpr int p_dudg = p_M + D::NPV * D::NPV;
-    static constexpr int p_end = p_dudg + D::NQ;
-    // assembly scratch
-    static constexpr int x_Xx = p_end;                            // [NGV, ND, ND]
-    static constexpr int x_jac = x_Xx + D::NGV * D::ND * D::ND;
-    static constexpr int x_nl = x_jac + D::NGV;                   // [NGT, ND]
-    static constexpr int x_jf = x_nl + D::NGT * D::ND;
-    static constexpr int x_sh = x_jf + D::NGT;                    // [NPV, NCU*ND] q part of SH
-    static constexpr int x_ug = x_sh + D::NPV * D::NCU * D::ND;   // [NGV, NC]
-    static constexpr int x_fu = x_ug + D::NGV * D::NC;            // [NGT, NC]
-    static constexpr int x_fuh = x_fu + D::NGT * D::NC;           // [NGT, NCU]
-    static constexpr int x_wrk = x_fuh + D::NGT * D::NCU;         // [NGV, ND, NCU]
-    static constexpr int x_wrl = x_wrk + D::NGV * D::ND * D::NCU; // [NGV, ND, NCU, NC]
-    static constexpr int x_FH = x_wrl + D::NGV * D::ND * D::NCU * D::NC;  // [NGT, NCU] jac*fhat
-    static constexpr int x_BH = x_FH + D::NGT * D::NCU;           // [NGT, NCU] jac*(fbou or fhat)
-    static constexpr int x_FHu = x_BH + D::NGT * D::NCU;          // [NGT, NCU, NC] jac*dfhat/dudg
-    static constexpr int x_FHh = x_FHu + D::NGT * D::NCU * D::NC; // [NGT, NCU, NCU] jac*dfhat/duh
-    static constexpr int x_Zc = x_FHh + D::NGT * D::NCU * D::NCU; // [NGV, NPV, ND]
-    static constexpr int x_Ze = x_Zc + (VISC ? D::NGV * D::NPV * D::ND : 0);   // [NGV, NDF, ND]
-    static constexpr int x_Zr = x_Ze + (VISC ? D::NGV * D::NDF * D::ND : 0);   // [NGV, NCU, ND]
-    static constexpr int x_ZFc = x_Zr + (VISC ? D::NGV * D::NCU * D::ND : 0);  // [NGT, NPV, ND]
-    static constexpr int x_ZFe = x_ZFc + (VISC ? D::NGT * D::NPV * D::ND : 0); // [NGT, NDF, ND]
-    static constexpr int x_ZFr = x_ZFe + (VISC ? D::NGT * D::NDF * D::ND : 0); // [NGT, NCU, ND]
-    static constexpr int x_end = x_ZFr + (VISC ? D::NGT * D::NCU * D::ND : 0);
-    static constexpr int x_size = x_end - p_end;
+    static constexpr int p_dudg = p_Rh + D::NH;
+    static constexpr int p_SDsep = p_dudg + D::NQ;                // SD when it does not fit the scratch
+    static constexpr int p_end = p_SDsep + (SD_ALIAS ? 0 : D::NU * D::NU);
+    static constexpr int p_SD = SD_ALIAS ? x_start : p_SDsep;
     // column tiles of DUDG_DUH (reuse the scratch)
     static constexpr int NCG = VISC ? D::NC : D::NCU;
     static constexpr int per_col = D::NQ + D::NGT * NCG + D::NGT * D::NCU;
     static constexpr int TILE_RAW = x_size / per_col;
     static constexpr int TILE = TILE_RAW < 1 ? 1 : (TILE_RAW > D::NH ? D::NH : TILE_RAW);
-    static constexpr int y_X = p_end;
+    static constexpr int y_X = x_start;
     static constexpr int y_Xg = y_X + D::NQ * TILE;
     static constexpr int y_Y = y_Xg + D::NGT * NCG * TILE;
     static constexpr int y_end = y_Y + D::NGT * D::NCU * TILE;
-    static constexpr int d_slots = (x_end > y_end ? x_end : y_end);   // 3 x u64 pivot slots
+    static_assert(y_end <= x_end, "the column tiles fit the scratch");
+    static constexpr int d_slots = p_end;                               // 3 x u64 pivot slots
     static constexpr int d_pcol = d_slots + 4;                          // [4*NU] pivot column copies
     static constexpr int d_diag = d_pcol + 4 * D::NU;                   // [NU] pivots
     static constexpr int d_b0 = d_diag + D::NU;                         // [NU] first right-hand side
-    static constexpr int d_inv = d_b0 + D::NU;                          // [NU*NU] FP32-accurate SD^-1 (MIXED)
-    static constexpr int n_doubles = d_inv + (MIXED ? D::NU * D::NU : 0);
+    static constexpr int d_invsep = d_b0 + D::NU;                       // [NU*NU] FP32-accurate SD^-1 (MIXED)
+    static constexpr int n_doubles = d_invsep + ((MIXED && !INV_ALIAS) ? D::NU * D::NU : 0);
+    static constexpr int d_inv = INV_ALIAS ? x_start + (SD_ALIAS ? D::NU * D::NU : 0) : d_invsep;
     // integers after the doubles
     static constexpr int i_perm = 0;                      // [NPF, NFE] 0-based
     static constexpr int i_invp = D::NPF * D::NFE;        // [NPV, NFE] face-local index or -1
@@ -124,8 +135,20 @@ struct Plan {
     static constexpr size_t bytes = sizeof(double) * n_doubles + sizeof(int) * n_ints;
 };
 
+// Resident elements per SM: the kernel is latency-bound (barrier-separated phases, a 40-step
+// elimination), so more elements in flight per SM beat more threads per element.  A plan that
+// fits four CTAs per SM runs four of 128 threads, one that fits three runs three of 192 (up to
+// 112 registers each); the larger plans run two or one of 256.  (C2, 2D NS p = 3: 6.84 ms
+// with two CTAs of 256, 6.21 ms with three of 192; 2D p = 2: 3.01 -> 1.80 ms with four of 128.)
 template <class D, bool VISC, bool MIXED>
-constexpr int min_blocks() { return Plan<D, VISC, MIXED>::bytes <= 110 * 1024 ? 2 : 1; }
+constexpr int min_blocks() {
+    return Plan<D, VISC, MIXED>::bytes <= 45 * 1024 ? 4
+         : (Plan<D, VISC, MIXED>::bytes <= 74 * 1024 ? 3 : (Plan<D, VISC, MIXED>::bytes <= 110 * 1024 ? 2 : 1));
+}
+template <class D, bool VISC, bool MIXED>
+constexpr int cta_threads() {
+    return min_blocks<D, VISC, MIXED>() == 4 ? 128 : (min_blocks<D, VISC, MIXED>() == 3 ? 192 : 256);
+}
 
 // MIXED: the local elimination of the Jacobian columns runs in FP32 (with the identity
 // appended so that the FP32 inverse of SD comes out too); the local residual solve (DUDG)
@@ -144,23 +167,20 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     int *si = reinterpret_cast<int *>(sm + L::n_doubles);
     const int tid = threadIdx.x;
 
-    double *t_vt = sm + L::t_vt, *t_vg = sm + L::t_vg, *t_mv = sm + L::t_mv;
-    double *t_ft = sm + L::t_ft, *t_fg = sm + L::t_fg, *t_mf = sm + L::t_mf;
+    double *t_vt = sm + L::t_vt, *t_vg = sm + L::t_vg;
+    double *t_ft = sm + L::t_ft, *t_fg = sm + L::t_fg;
+    const double *__restrict__ t_mv = P.shapmv;   // geometry tables: read once per element from L1
+    const double *__restrict__ t_mf = P.shapmf;
     int *perm = si + L::i_perm, *invp = si + L::i_invp;
 
     // ---- master tables, once per CTA
     for (int i = tid; i < NGV * NPV * (ND + 1); i += NT) {
         t_vt[i] = P.shapvt[i];
         t_vg[i] = P.shapvg[i];
-        t_mv[i] = P.shapmv[i];
     }
     for (int i = tid; i < NGF * NPF; i += NT) {
         t_ft[i] = P.shapft[i];   // value slice of shapft[ngf,npf,nd]
         t_fg[i] = P.shapfg[i];   // value slice of shapfg[npf,ngf,nd]
-    }
-    for (int i = tid; i < NGF * NPF * ND; i += NT) {
-        const int g = i % NGF, n = (i / NGF) % NPF, k = i / (NGF * NPF);
-        t_mf[i] = P.shapmf[g + NGF * (n + NPF * k)];
     }
     for (int i = tid; i < NPF * NFE; i += NT) perm[i] = P.perm[i] - 1;
     for (int i = tid; i < NPV * NFE; i += NT) invp[i] = -1;
@@ -174,7 +194,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     double *s_Gp = sm + L::p_Gp, *s_Hp = sm + L::p_Hp, *s_Rh = sm + L::p_Rh, *s_M = sm + L::p_M;
     double *s_dudg = sm + L::p_dudg;
     double *x_Xx = sm + L::x_Xx, *x_jac = sm + L::x_jac, *x_nl = sm + L::x_nl, *x_jf = sm + L::x_jf;
-    double *x_sh = sm + L::x_sh, *x_ug = sm + L::x_ug, *x_fu = sm + L::x_fu, *x_fuh = sm + L::x_fuh;
+    double *x_ug = sm + L::x_ug, *x_fu = sm + L::x_fu, *x_fuh = sm + L::x_fuh;
     double *x_wrk = sm + L::x_wrk, *x_wrl = sm + L::x_wrl, *x_FH = sm + L::x_FH, *x_BH = sm + L::x_BH;
     double *x_FHu = sm + L::x_FHu, *x_FHh = sm + L::x_FHh;
     double *x_Zc = sm + L::x_Zc, *x_Ze = sm + L::x_Ze, *x_Zr = sm + L::x_Zr;
@@ -185,16 +205,17 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     double *s_pcol = sm + L::d_pcol, *s_diag = sm + L::d_diag;
 
     for (int e = blockIdx.x; e < P.ne; e += gridDim.x) {
+        bool force_piv = false;      // set when the unpivoted solve failed its check and SD sits on
+                                     // the scratch: the element is then evaluated again, pivoted
+    elem_start:
         // ================================================================ load
         {
             const double *g_dg = P.dgnodes + (size_t)e * NPV * ND;
             const double *g_udg = P.UDG + (size_t)e * NPV * NC;
             const double *g_uh = P.UH + (size_t)e * NCU * NDF;
-            const double *g_sh = P.SH + (size_t)e * NPV * NC;
             for (int i = tid; i < NPV * ND; i += NT) s_dg[i] = g_dg[i];
             for (int i = tid; i < NPV * NC; i += NT) s_udg[i] = g_udg[i];
             for (int i = tid; i < NCU * NDF; i += NT) s_uh[i] = g_uh[i];
-            for (int i = tid; i < NPV * NCU * ND; i += NT) x_sh[i] = g_sh[NPV * NCU + i];
             if (tid < NFE) s_bf[tid] = P.bf[(size_t)e * NFE + tid];
             if (tid == 0) *s_bad = 0;
         }
@@ -322,13 +343,14 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         }
         __syncthreads();
         // Rq = M (SH/fc_q - q) + C u - E uh   (volint.m:57-60, faceint.m:49-51)
+        const double *__restrict__ g_shq = P.SH + (size_t)e * NPV * NC + NPV * NCU;   // q part of SH
         for (int i = tid; i < NPV * NCU * ND; i += NT) {
             const int r = i % NPV, a = (i / NPV) % NCU, d = i / (NPV * NCU);
             const int cq = NCU + a + NCU * d;
             double t = 0.0;
 #pragma unroll
             for (int s = 0; s < NPV; s++)
-                t += s_M[r + NPV * s] * (x_sh[s + NPV * (a + NCU * d)] / P.fc_q - s_udg[s + NPV * cq]);
+                t += s_M[r + NPV * s] * (g_shq[s + NPV * (a + NCU * d)] / P.fc_q - s_udg[s + NPV * cq]);
 #pragma unroll
             for (int s = 0; s < NPV; s++) t += s_MiC[r + NPV * (s + NPV * d)] * s_udg[s + NPV * a];
             for (int f = 0; f < NDF; f++) t -= s_MiE[r + NPV * (f + NDF * d)] * s_uh[a + NCU * f];
@@ -482,6 +504,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             const int kf = kk - KV, j = kf / NGF, g = kf % NGF, m = invp[r + NPV * j];
             return m >= 0 ? t_fg[m + NPF * g] : 0.0;
         };
+        auto build_sd = [&]() {
         tile_gemm<NCU * NCU, NPV, NPV, KK, TMS, 2, NT, 2>(
             phi,
             [&](int ab, int kk, int k) -> double {
@@ -509,6 +532,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                 const int a = ab % NCU, b = ab / NCU;
                 s_SD[(r + NPV * a) + NU * (k + NPV * b)] = v;
             });
+        };
         auto build_rhs = [&]() {
         // rhs0 = Ru - B Mi Rq (volint.m:258, faceint.m:306-331; schur_primal.m:95,111)
         for (int i = tid; i < NU; i += NT) {
@@ -582,12 +606,17 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             for (int g = 0; g < NGF; g++) t += t_fg[m + NPF * g] * x_BH[(g + NGF * j) + NGT * a];
             s_Rh[i] = -t;
         }
+        if constexpr (L::SD_ALIAS) __syncthreads();     // SD overwrites what the RHS and Rh read
+        build_sd();
         __syncthreads();
 
         // ================================ LU of SD and the 1 + NH solves (schur_primal.m:111,118)
         {
             int bad_before = *s_bad;
             __syncthreads();
+            if (force_piv) {
+                gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
+            } else {
             // Unpivoted elimination with the density unknowns last (in natural order interior
             // nodes have structurally zero density pivots: the continuity flux does not depend on
             // the density), accepted when the backward error of the first column,
@@ -664,9 +693,16 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             }
             if (s_gslot[0]) {
                 // fall back to partial pivoting on the original system
-                build_rhs();
-                __syncthreads();
-                gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
+                if (L::SD_ALIAS) {
+                    force_piv = true;            // the right-hand sides' inputs are overwritten by SD
+                    __syncthreads();
+                    goto elem_start;
+                } else {
+                    build_rhs();
+                    __syncthreads();
+                    gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
+                }
+            }
             }
             if (tid == 0 && *s_bad && !bad_before) *s_bad = 2;
             __syncthreads();
@@ -795,7 +831,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
 // ------------------------------------------------------------------ dispatch
 template <class D, bool VISC, bool MIXED>
 static int launch_t(const ElemParams &p, cudaStream_t st, int grid_req) {
-    constexpr int NT = 256;
+    constexpr int NT = cta_threads<D, VISC, MIXED>();
     using L = Plan<D, VISC, MIXED>;
     static_assert(L::TILE >= 1, "tile");
     const size_t smem = L::bytes;

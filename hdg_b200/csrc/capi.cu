@@ -39,6 +39,7 @@ const char *hdgx_status_str(int code) {
         case -12: return "kernel launch failed";
         case -13: return "CUDA error while counting status";
         case -14: return "a flag-synchronised BILU(0) sweep gave up waiting (bounded spin)";
+        case -15: return "the fused Gram-Schmidt step gave up waiting at a grid barrier (bounded spin)";
         default:
             if (code <= -1000) return cudaGetErrorString((cudaError_t)(-1000 - code));
             return "unknown status";

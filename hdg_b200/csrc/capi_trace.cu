@@ -140,6 +140,29 @@ static int bilu0_apply(const hdgx_bsr *A, const double *Mg, const double *x, dou
     return launched();
 }
 
+__global__ void mgs_coop_kernel(size_t, int, const double *, double *, double *, double *, unsigned *, int *);
+
+// The Arnoldi orthogonalisation of w against V(:, 0:nv) and its normalisation as one cooperative
+// launch (mgs_coop_kernel); false when the device cannot hold the grid at once (the caller then
+// issues the separate products).  part: 2 * 1024 doubles; bar: 2 unsigned (bar[0] == 0 on entry).
+static bool mgs_fused(size_t n, int nv, const double *V, double *w, double *hcol, double *part, unsigned *bar, int *err,
+                      cudaStream_t st) {
+    unsigned grid = grid_for(n, 256);
+    if (grid > 1024) grid = 1024;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)mgs_coop_kernel, 256, 0) != cudaSuccess ||
+        (long long)per_sm * sm_count() < (long long)grid) {
+        cudaGetLastError();
+        return false;
+    }
+    void *args[] = {&n, &nv, &V, &w, &hcol, &part, &bar, &err};
+    if (cudaLaunchCooperativeKernel((const void *)mgs_coop_kernel, dim3(grid), dim3(256), args, 0, st) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
 // dot(a,b) -> *out (device); part: scratch of >= 1024 doubles
 static void dot(size_t n, const double *a, const double *b, double *out, double *part, int do_sqrt, cudaStream_t st) {
     const int threads = 256;
@@ -241,7 +264,7 @@ size_t hdgx_gmres_workspace_bytes(const hdgx_bsr *A, int restart) {
     if (!A || restart < 1) return 0;
     const size_t N = (size_t)A->bs * A->nf;
     const size_t m = (size_t)restart;
-    return sizeof(double) * (N * (m + 1) + 3 * N + (m + 1) * m + 4 * (m + 1) + 8 + 1024) + 256;
+    return sizeof(double) * (N * (m + 1) + 3 * N + (m + 1) * m + 4 * (m + 1) + 8 + 2048 + 2) + 256;
 }
 
 int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, const double *b, double *x, int restart,
@@ -266,7 +289,10 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
     gs.g = gs.sn + (m + 1);
     gs.y = gs.g + (m + 1);
     gs.scal = gs.y + (m + 1);
-    double *part = gs.scal + 8;
+    double *part = gs.scal + 8;                   // [2048] partial sums
+    unsigned *bar = reinterpret_cast<unsigned *>(part + 2048);   // grid barrier of the fused step
+    int *bar_err = reinterpret_cast<int *>(bar + 1) + 1;         // [0] count, [1] generation, err
+    cudaMemsetAsync(bar, 0, 3 * sizeof(unsigned), st);
     // host scalars on the stack (pageable copies are stream-ordered and, unlike freeing
     // pinned memory, never synchronise the other streams of the device)
     double h_scal[2] = {0.0, 0.0};
@@ -296,12 +322,14 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
             rc |= matvec(A, Hg, vj, t, st);
             rc |= bilu0_apply(A, Mg, t, w2, w, st);
             double *hc = gs.H + (size_t)(m + 1) * j;
-            for (int i = 0; i <= j; i++) {            // modified Gram-Schmidt (gmres_bilu0.m:59-63)
-                dot(N, V + N * i, w, hc + i, part, 0, st);
-                axpy_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, hc + i, -1.0, V + N * i, w);
+            if (!mgs_fused(N, j + 1, V, w, hc, part, bar, bar_err, st)) {
+                for (int i = 0; i <= j; i++) {        // modified Gram-Schmidt (gmres_bilu0.m:59-63)
+                    dot(N, V + N * i, w, hc + i, part, 0, st);
+                    axpy_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, hc + i, -1.0, V + N * i, w);
+                }
+                dot(N, w, w, hc + j + 1, part, 1, st);
+                scale_div_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, hc + j + 1, w, w);
             }
-            dot(N, w, w, hc + j + 1, part, 1, st);
-            scale_div_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, hc + j + 1, w, w);
             givens_kernel<<<1, 1, 0, st>>>(gs, m, j);
             cudaMemcpyAsync(h_res, gs.scal + 1, sizeof(double), cudaMemcpyDeviceToHost, st);
             cudaStreamSynchronize(st);
@@ -322,6 +350,9 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
     if (iters) *iters = iter;
     if (flag) *flag = fl;
     if (relres) *relres = res_rel;
+    int mgs_err = 0;
+    cudaMemcpyAsync(&mgs_err, bar_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
     int sched_err = 0;
     if (A->ncolors == 0 && A->sched) {
         cudaMemcpy(&sched_err, A->sched + 2, sizeof(int), cudaMemcpyDeviceToHost);
@@ -330,6 +361,7 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
     if (own) cudaFreeAsync(mem, st);
     if (cudaGetLastError() != cudaSuccess) return -12;
     if (sched_err) return -14;
+    if (mgs_err) return -15;
     return rc ? -12 : 0;
 }
 

@@ -429,6 +429,83 @@ template __global__ void block_norms_kernel<256>(int, int, const long long *, co
 // after which the error flag is raised and the row proceeds.
 #define HDGX_SPIN_LIMIT (1 << 22)
 
+// ------------------------------------------------------------- fused Gram-Schmidt step
+// Blocks of one cooperative launch meet here.  Thread 0 of each block arrives on a counter; the
+// last one resets it and advances the generation; the others poll the generation with a bounded
+// wait (after HDGX_SPIN_LIMIT polls the error flag is raised and the block goes on).
+__device__ __forceinline__ void grid_barrier(unsigned *bar, unsigned nblocks, int *err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == nblocks - 1) {
+            bar[0] = 0;
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            int n = 0;
+            while (*gen == g) {
+                if (++n > HDGX_SPIN_LIMIT) { atomicExch(err, 1); break; }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// One Arnoldi orthogonalisation of GMRES (modified Gram-Schmidt, gmres_bilu0.m:59-63: for
+// i < nv, h_i = v_i . w, w -= h_i v_i; then h_nv = |w|, w /= h_nv) as ONE cooperative launch
+// instead of 3 (nv + 1) small ones.  The grid is that of the two-pass dot product it replaces,
+// each block forms its partial sums over the same grid-stride elements and every block adds the
+// partials in the order of dot_final_kernel (256 threads), so the results are the same bit for
+// bit; every element of w is read and written by the same thread throughout, so one grid
+// barrier per product suffices (partials alternate between two halves of part[2 * grid]).
+__global__ void __launch_bounds__(256) mgs_coop_kernel(size_t n, int nv, const double *__restrict__ V, double *w,
+                                                       double *hcol, double *part, unsigned *bar, int *err) {
+    __shared__ double red[32];
+    __shared__ double hval;
+    const unsigned G = gridDim.x;
+    const int tid = threadIdx.x;
+    for (int i = 0; i <= nv; i++) {
+        const double *a = i < nv ? V + n * i : w;
+        double *pp = part + (size_t)(i & 1) * G;
+        double s = 0.0;
+        for (size_t t = blockIdx.x * (size_t)blockDim.x + tid; t < n; t += (size_t)G * blockDim.x) s += a[t] * w[t];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((tid & 31) == 0) red[tid >> 5] = s;
+        __syncthreads();
+        if (tid < 32) {
+            s = (tid < (int)(blockDim.x >> 5)) ? red[tid] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (tid == 0) pp[blockIdx.x] = s;
+        }
+        grid_barrier(bar, G, err);
+        s = 0.0;
+        for (int t = tid; t < (int)G; t += blockDim.x) s += __ldcg(pp + t);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((tid & 31) == 0) red[tid >> 5] = s;
+        __syncthreads();
+        if (tid == 0) {
+            double r = 0.0;
+            for (int q = 0; q < (int)(blockDim.x >> 5); q++) r += red[q];
+            hval = (i < nv) ? r : sqrt(r);
+            if (blockIdx.x == 0) hcol[i] = hval;
+        }
+        __syncthreads();
+        const double h = hval;
+        if (i < nv) {
+            const double al = -1.0 * h;
+            for (size_t t = blockIdx.x * (size_t)blockDim.x + tid; t < n; t += (size_t)G * blockDim.x) w[t] += al * a[t];
+        } else {
+            const double sc = (h != 0.0) ? 1.0 / h : 0.0;
+            for (size_t t = blockIdx.x * (size_t)blockDim.x + tid; t < n; t += (size_t)G * blockDim.x) w[t] = w[t] * sc;
+        }
+        __syncthreads();
+    }
+}
+
 __device__ __forceinline__ int load_acquire(const int *p) {
     int v;
     asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");

@@ -54,12 +54,13 @@ struct Dims {
 // is dead during the solve).  The geometry tables shapmv / shapmf are read from global
 // memory (L1) instead: they are used once per element.  Less shared memory per element means
 // more elements resident per SM (the kernel is latency-bound).
-template <class D, bool VISC, bool MIXED = false>
+template <class D, bool VISC, bool MIXED = false, bool TAB = true>
 struct Plan {
-    // master tables (loaded once per CTA)
+    // master tables (loaded once per CTA; shapvt / shapvg stay in global memory when !TAB)
+    static constexpr bool TABLES = TAB;
     static constexpr int t_vt = 0;
-    static constexpr int t_vg = t_vt + D::NGV * D::NPV * (D::ND + 1);
-    static constexpr int t_ft = t_vg + D::NPV * D::NGV * (D::ND + 1);
+    static constexpr int t_vg = t_vt + (TAB ? D::NGV * D::NPV * (D::ND + 1) : 0);
+    static constexpr int t_ft = t_vg + (TAB ? D::NPV * D::NGV * (D::ND + 1) : 0);
     static constexpr int t_fg = t_ft + D::NGF * D::NPF;
     // assembly scratch, first group: not read by the SD build
     static constexpr int x_start = t_fg + D::NPF * D::NGF;
@@ -140,11 +141,16 @@ struct Plan {
 // fits four CTAs per SM runs four of 128 threads, one that fits three runs three of 192 (up to
 // 112 registers each); the larger plans run two or one of 256.  (C2, 2D NS p = 3: 6.84 ms
 // with two CTAs of 256, 6.21 ms with three of 192; 2D p = 2: 3.01 -> 1.80 ms with four of 128.)
-template <class D, bool VISC, bool MIXED>
-constexpr int min_blocks() {
-    return Plan<D, VISC, MIXED>::bytes <= 45 * 1024 ? 4
-         : (Plan<D, VISC, MIXED>::bytes <= 74 * 1024 ? 3 : (Plan<D, VISC, MIXED>::bytes <= 110 * 1024 ? 2 : 1));
+// The volume tables shapvt / shapvg move from shared to global memory (read through L1) only
+// when that raises the number of resident CTAs (2D p = 4: 119 -> 108 KB, one -> two per SM).
+constexpr int blocks_for(size_t bytes) {
+    return bytes <= 45 * 1024 ? 4 : (bytes <= 74 * 1024 ? 3 : (bytes <= 110 * 1024 ? 2 : 1));
 }
+template <class D, bool VISC, bool MIXED>
+using PlanSel = Plan<D, VISC, MIXED,
+                     (blocks_for(Plan<D, VISC, MIXED, false>::bytes) <= blocks_for(Plan<D, VISC, MIXED, true>::bytes))>;
+template <class D, bool VISC, bool MIXED>
+constexpr int min_blocks() { return blocks_for(PlanSel<D, VISC, MIXED>::bytes); }
 template <class D, bool VISC, bool MIXED>
 constexpr int cta_threads() {
     return min_blocks<D, VISC, MIXED>() == 4 ? 128 : (min_blocks<D, VISC, MIXED>() == 3 ? 192 : 256);
@@ -157,7 +163,7 @@ constexpr int cta_threads() {
 // changes the Newton convergence rate, not the converged solution).
 template <class D, bool VISC, bool MIXED, int NT>
 __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_kernel(const __grid_constant__ ElemParams P) {
-    using L = Plan<D, VISC, MIXED>;
+    using L = PlanSel<D, VISC, MIXED>;
     constexpr int ND = D::ND, NPV = D::NPV, NPF = D::NPF, NGV = D::NGV, NGF = D::NGF;
     constexpr int NFE = D::NFE, NCU = D::NCU, NC = D::NC, NDF = D::NDF, NU = D::NU;
     constexpr int NQ = D::NQ, NH = D::NH, NGT = D::NGT;
@@ -167,16 +173,18 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     int *si = reinterpret_cast<int *>(sm + L::n_doubles);
     const int tid = threadIdx.x;
 
-    double *t_vt = sm + L::t_vt, *t_vg = sm + L::t_vg;
+    const double *t_vt = L::TABLES ? sm + L::t_vt : P.shapvt, *t_vg = L::TABLES ? sm + L::t_vg : P.shapvg;
     double *t_ft = sm + L::t_ft, *t_fg = sm + L::t_fg;
     const double *__restrict__ t_mv = P.shapmv;   // geometry tables: read once per element from L1
     const double *__restrict__ t_mf = P.shapmf;
     int *perm = si + L::i_perm, *invp = si + L::i_invp;
 
     // ---- master tables, once per CTA
-    for (int i = tid; i < NGV * NPV * (ND + 1); i += NT) {
-        t_vt[i] = P.shapvt[i];
-        t_vg[i] = P.shapvg[i];
+    if constexpr (L::TABLES) {
+        for (int i = tid; i < NGV * NPV * (ND + 1); i += NT) {
+            sm[L::t_vt + i] = P.shapvt[i];
+            sm[L::t_vg + i] = P.shapvg[i];
+        }
     }
     for (int i = tid; i < NGF * NPF; i += NT) {
         t_ft[i] = P.shapft[i];   // value slice of shapft[ngf,npf,nd]
@@ -832,7 +840,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
 template <class D, bool VISC, bool MIXED>
 static int launch_t(const ElemParams &p, cudaStream_t st, int grid_req) {
     constexpr int NT = cta_threads<D, VISC, MIXED>();
-    using L = Plan<D, VISC, MIXED>;
+    using L = PlanSel<D, VISC, MIXED>;
     static_assert(L::TILE >= 1, "tile");
     const size_t smem = L::bytes;
     if (smem > 227 * 1024) return -3;

@@ -35,6 +35,13 @@ __device__ __forceinline__ void cluster_arrive_relaxed() {
 __device__ __forceinline__ void cluster_wait_acquire() {
     asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+// the 16-byte aligned interior of [p, p + bytes) into L2 (a bulk prefetch needs aligned ends)
+__device__ __forceinline__ void bulk_prefetch_l2(const void *p, unsigned bytes) {
+    const unsigned long long a0 = ((unsigned long long)p + 15) & ~15ull;
+    const unsigned long long a1 = ((unsigned long long)p + bytes) & ~15ull;
+    if (a1 > a0) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"((unsigned)(a1 - a0)) : "memory");
+}
 
 // One row component's record and (PL) matrix values, loadable ahead of the level that uses them.
 template <int BS, int MAXD, bool PL, bool DIAG>
@@ -148,9 +155,34 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NT)
         const int q0 = lp[lev], nr = lp[lev + 1] - q0, s = rank + CS * m;
         return (m < RPP && s < nr) ? rec + (size_t)(q0 + s) * RW : nullptr;
     };
+    // L2 pipeline for the first pass of later levels (the factors are read once per apply and
+    // do not stay in L2 between applies): the records of level lev + DR are prefetched to L2;
+    // one block index per thread (component r < NK of the row: a neighbour block, in the
+    // backward sweep r = 0 the diagonal block) is loaded DK levels ahead and its block
+    // prefetched to L2 one level later, so the register prefetch of the next level hits L2.
+    constexpr int DR = 7, DK = 4;
+    auto prefetch_rec = [&](int lev) {
+        if (r == 0 && lev >= 0 && lev < nlev) {
+            const int *R = slot_rec(lev);
+            if (R) { prefetch_l2(R); prefetch_l2(R + RW - 1); }
+        }
+    };
+    // the block index component r prefetches at level lev (-1: none); BWD: backward-sweep blocks
+    auto block_of = [&](int lev, bool bwd) -> int {
+        if (lev < 0 || lev >= nlev) return -1;
+        const int *R = slot_rec(lev);
+        if (!R) return -1;
+        if (!bwd) return r < MAXD ? __ldcg(R + 2 + 2 * r) : -1;
+        return r == 0 ? __ldcg(R + 1) : (r <= MAXD ? __ldcg(R + 2 + 2 * MAXD + 2 * (r - 1)) : -1);
+    };
+    auto prefetch_block = [&](int k) {
+        if (k >= 0) bulk_prefetch_l2(Mg + (size_t)BS * BS * k, (unsigned)(sizeof(double) * BS * BS));
+    };
 
     // forward sweep: y_i = x_i - sum_{j before i} L_ij y_j, levels in elimination order
     {
+        for (int l = 0; l < DR; l++) prefetch_rec(l);
+        int pk = block_of(DK - 1, false);
         RowPrefetch<BS, MAXD, PLF, false> pf;
         pf.template load<0>(slot_rec(0), Mg, r);
         double xv = pf.i >= 0 ? __ldg(x + (size_t)BS * pf.i + r) : 0.0;
@@ -171,11 +203,16 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NT)
                 pf.template load<0>(slot_rec(lev + 1), Mg, r);
                 xv = pf.i >= 0 ? __ldg(x + (size_t)BS * pf.i + r) : 0.0;
             }
+            prefetch_block(pk);                         // level lev + DK - 1
+            pk = block_of(lev + DK, false);
+            prefetch_rec(lev + DR);
             cluster_wait_acquire();
         }
     }
     // backward sweep: v_i = inv(U_ii) (y_i - sum_{j after i} U_ij v_j), levels in reverse order
     {
+        for (int l = 0; l < DR; l++) prefetch_rec(nlev - 1 - l);
+        int pk = block_of(nlev - DK, true);
         RowPrefetch<BS, MAXD, PLB, true> pf;
         pf.template load<2 * MAXD>(slot_rec(nlev - 1), Mg, r);
         for (int lev = nlev - 1; lev >= 0; lev--) {
@@ -199,6 +236,9 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NT)
             __threadfence();
             cluster_arrive_relaxed();
             if (lev > 0) pf.template load<2 * MAXD>(slot_rec(lev - 1), Mg, r);
+            prefetch_block(pk);                         // level lev - DK + 1
+            pk = block_of(lev - DK, true);
+            prefetch_rec(lev - DR);
             cluster_wait_acquire();
         }
     }

@@ -97,6 +97,8 @@ def _declare(L):
     L.hdgx_elemental.argtypes = [p(HdgxMaster), p(HdgxApp), i] + [v] * 10 + [v]
     L.hdgx_elemental_mixed.restype = i
     L.hdgx_elemental_mixed.argtypes = [p(HdgxMaster), p(HdgxApp), i] + [v] * 10 + [v]
+    L.hdgx_elemental_host.restype = i
+    L.hdgx_elemental_host.argtypes = [p(HdgxMaster), p(HdgxApp), i] + [v] * 10 + [i, i, v]
     L.hdgx_schur_uq.restype = i
     L.hdgx_schur_uq.argtypes = [i] * 5 + [v] * 15 + [v]
     L.hdgx_schur_u.restype = i

@@ -9,6 +9,7 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
                      const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
                      double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed,
                      int grid);
+cudaMemPool_t device_pool();
 int schur_launch(int qform, int nd, int npv, int ncu, int nc, int ndf, int ne, const double *M,
                  const double *C, const double *E, const double *BD, const double *F, const double *GK,
                  const double *H, const double *Rq, const double *Ru, const double *Rh, double *DUDG,
@@ -165,6 +166,111 @@ int hdgx_elemental_buckets(int nb, const hdgx_elem_bucket *b, int mixed, hdgx_st
         if (cudaEventRecord(fs->join[si], fs->s[si]) != cudaSuccess && !rc) rc = -12;
         if (cudaStreamWaitEvent(st, fs->join[si], 0) != cudaSuccess && !rc) rc = -12;
     }
+    return rc;
+}
+
+// Host-array form: the elements go through two device staging sets in chunks, and chunk c's
+// upload (stream s_in), chunk c-1's kernel (the caller's stream) and chunk c-2's download
+// (stream s_out) run at the same time.  Set b = c % 2 is reused by chunk c + 2 only after
+// chunk c's kernel has read its inputs (upload waits on ev_k[b]) and chunk c's download has
+// read its outputs (kernel waits on ev_out[b]).
+int hdgx_elemental_host(const hdgx_master *master, const hdgx_app *app, int ne, const double *dgnodes,
+                        const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
+                        double *FE, double *DUDG, double *DUDG_DUH, int *status, int mixed, int chunk,
+                        hdgx_stream_t stream) {
+    if (int rc = check_elemental(master, app, ne, dgnodes, bf, UDG, UH, SH, AE, FE, DUDG, DUDG_DUH)) return rc;
+    if (chunk < 0) return -1;
+    if (ne == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t npv = master->npv, nd = master->nd, nfe = master->nfe, nc = app->nc, ncu = app->ncu;
+    const size_t ndf = (size_t)master->npf * nfe;
+    // doubles (ints for bf, status) per element of every array, in argument order
+    const size_t n_x = npv * nd, n_u = npv * nc, n_h = ncu * ndf, n_ae = n_h * n_h, n_dd = n_u * n_h;
+    if (chunk == 0) chunk = ne < 16 * 1024 ? (ne < 1024 ? ne : 1024) : (ne + 15) / 16;
+    if (chunk > ne) chunk = ne;
+    // one staging set: every array of `chunk` elements, each on a 256-byte boundary
+    const size_t dbl[8] = {n_x, n_u, n_h, n_u, n_ae, n_h, n_u, n_dd}, ints[2] = {nfe, 1};
+    auto rnd = [](size_t bytes) { return (bytes + 255) & ~(size_t)255; };
+    size_t set_bytes = 0;
+    for (size_t d : dbl) set_bytes += rnd(sizeof(double) * d * chunk);
+    for (size_t d : ints) set_bytes += rnd(sizeof(int) * d * chunk);
+    cudaMemPool_t pool = hdgx::device_pool();
+    if (!pool) return -12;
+    unsigned char *stage = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync((void **)&stage, 2 * set_bytes, pool, st);
+    if (e != cudaSuccess) return -1000 - (int)e;
+    struct Set { double *x, *u, *h, *s, *ae, *fe, *dd, *ddh; int *bf, *status; } set[2];
+    for (int b = 0; b < 2; b++) {
+        unsigned char *p = stage + b * set_bytes;
+        double **dp[8] = {&set[b].x, &set[b].u, &set[b].h, &set[b].s, &set[b].ae, &set[b].fe, &set[b].dd, &set[b].ddh};
+        for (int k = 0; k < 8; k++) { *dp[k] = (double *)p; p += rnd(sizeof(double) * dbl[k] * chunk); }
+        set[b].bf = (int *)p;
+        p += rnd(sizeof(int) * nfe * chunk);
+        set[b].status = (int *)p;
+    }
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_done = nullptr, ev_in[2] = {}, ev_k[2] = {}, ev_out[2] = {};
+    int rc = 0;
+    auto ok = [&](cudaError_t r) { if (r != cudaSuccess && !rc) rc = -1000 - (int)r; return rc == 0; };
+    ok(cudaStreamCreateWithFlags(&s_in, cudaStreamNonBlocking));
+    ok(cudaStreamCreateWithFlags(&s_out, cudaStreamNonBlocking));
+    ok(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming));
+    ok(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+    for (int b = 0; b < 2; b++) {
+        ok(cudaEventCreateWithFlags(&ev_in[b], cudaEventDisableTiming));
+        ok(cudaEventCreateWithFlags(&ev_k[b], cudaEventDisableTiming));
+        ok(cudaEventCreateWithFlags(&ev_out[b], cudaEventDisableTiming));
+    }
+    if (rc == 0) {
+        ok(cudaEventRecord(ev_start, st));                  // the staging allocation is ordered on st
+        ok(cudaStreamWaitEvent(s_in, ev_start, 0));
+        ok(cudaStreamWaitEvent(s_out, ev_start, 0));
+        const int nch = (ne + chunk - 1) / chunk;
+        for (int c = 0; c < nch && rc == 0; c++) {
+            const int b = c & 1;
+            const size_t e0 = (size_t)c * chunk;
+            const int n = (int)((size_t)ne - e0 < (size_t)chunk ? (size_t)ne - e0 : (size_t)chunk);
+            const Set &S = set[b];
+            auto h2d = [&](void *dst, const void *src, size_t per) {
+                return ok(cudaMemcpyAsync(dst, (const unsigned char *)src + per * e0, per * n, cudaMemcpyHostToDevice, s_in));
+            };
+            auto d2h = [&](void *dst, const void *src, size_t per) {
+                return ok(cudaMemcpyAsync((unsigned char *)dst + per * e0, src, per * n, cudaMemcpyDeviceToHost, s_out));
+            };
+            if (c >= 2) ok(cudaStreamWaitEvent(s_in, ev_k[b], 0));
+            h2d(S.x, dgnodes, sizeof(double) * n_x);
+            h2d(S.bf, bf, sizeof(int) * nfe);
+            h2d(S.u, UDG, sizeof(double) * n_u);
+            h2d(S.h, UH, sizeof(double) * n_h);
+            h2d(S.s, SH, sizeof(double) * n_u);
+            ok(cudaEventRecord(ev_in[b], s_in));
+            ok(cudaStreamWaitEvent(st, ev_in[b], 0));
+            if (c >= 2) ok(cudaStreamWaitEvent(st, ev_out[b], 0));
+            if (rc) break;
+            const int r = hdgx::elemental_launch(master, app, n, S.x, S.bf, S.u, S.h, S.s, S.ae, S.fe, S.dd, S.ddh,
+                                                 status ? S.status : nullptr, st, mixed != 0, 0);
+            if (r) { rc = r; break; }
+            ok(cudaEventRecord(ev_k[b], st));
+            ok(cudaStreamWaitEvent(s_out, ev_k[b], 0));
+            d2h(AE, S.ae, sizeof(double) * n_ae);
+            d2h(FE, S.fe, sizeof(double) * n_h);
+            d2h(DUDG, S.dd, sizeof(double) * n_u);
+            d2h(DUDG_DUH, S.ddh, sizeof(double) * n_dd);
+            if (status) d2h(status, S.status, sizeof(int));
+            ok(cudaEventRecord(ev_out[b], s_out));
+        }
+        // join the copy streams back into st (also after a failure), then release the staging
+        cudaEventRecord(ev_done, s_in);
+        cudaStreamWaitEvent(st, ev_done, 0);
+        cudaEventRecord(ev_done, s_out);
+        cudaStreamWaitEvent(st, ev_done, 0);
+    }
+    cudaFreeAsync(stage, st);
+    ok(cudaStreamSynchronize(st));
+    if (s_in) cudaStreamDestroy(s_in);
+    if (s_out) cudaStreamDestroy(s_out);
+    for (cudaEvent_t ev : {ev_start, ev_done, ev_in[0], ev_in[1], ev_k[0], ev_k[1], ev_out[0], ev_out[1]})
+        if (ev) cudaEventDestroy(ev);
     return rc;
 }
 

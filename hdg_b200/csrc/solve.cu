@@ -226,6 +226,9 @@ double norm2(size_t n, const double *x, double *part, double *out, cudaStream_t 
 }
 
 }  // namespace
+
+// the same private pool for the other entry points that stage data on the device
+cudaMemPool_t device_pool() { return solve_pool(); }
 }  // namespace hdgx
 
 using namespace hdgx;

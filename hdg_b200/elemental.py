@@ -154,6 +154,52 @@ def hdg_elemental(master, app, dgnodes, bf, UDG, UH, SH, out=None, stream=None, 
     return o
 
 
+def as_host_darray(x, dtype=torch.float64):
+    """A column-major page-locked host DArray of ``x`` (a numpy array, or a host DArray kept as is)."""
+    if isinstance(x, DArray):
+        if x.t.is_cuda:
+            raise HdgxError("expected a host array, got device memory")
+        if x.t.dtype != dtype:
+            raise TypeError(f"expected {dtype}, got {x.t.dtype}")
+        return x
+    a = np.asarray(x)
+    t = torch.from_numpy(np.ascontiguousarray(a.ravel(order="F"))).to(dtype).pin_memory()
+    return DArray(t, tuple(a.shape))
+
+
+def alloc_host_outputs(master, app, ne):
+    """Page-locked host outputs of hdg_elemental_host."""
+    npv, ncu, nc = master.npv, app.ncu, app.nc
+    ndf = master.npf * master.nfe
+
+    def pinned(shape, dtype=torch.float64):
+        return DArray(torch.empty(int(np.prod(shape)), dtype=dtype, pin_memory=True), tuple(int(x) for x in shape))
+    return ElementalOutputs(pinned((ncu, ndf, ncu, ndf, ne)), pinned((ncu, ndf, ne)), pinned((npv, nc, ne)),
+                            pinned((npv, nc, ncu, ndf, ne)), pinned((ne,), torch.int32))
+
+
+def hdg_elemental_host(master, app, dgnodes, bf, UDG, UH, SH, out=None, stream=None, dmaster=None, mixed=False,
+                       chunk=0):
+    """kernel/hdg_elemental.m on HOST arrays, as the reference is called: the per-element inputs
+    and outputs stay in page-locked host memory and the library streams them through the GPU in
+    chunks of ``chunk`` elements (0: its default), overlapping the uploads, the kernel and the
+    downloads.  Arguments as ``hdg_elemental``; returns ``ElementalOutputs`` of host ``DArray``s,
+    bitwise equal to the device-array call's.  Returns when the outputs are in host memory."""
+    _require_cuda()
+    L = lib()
+    dm = dmaster if dmaster is not None else DeviceMaster(master)
+    dg, udg, uh, sh = (as_host_darray(x) for x in (dgnodes, UDG, UH, SH))
+    bfh = as_host_darray(bf, dtype=torch.int32)
+    ne = udg.shape[-1]
+    o = out if out is not None else alloc_host_outputs(master, app, ne)
+    a = app_struct(app)
+    rc = L.hdgx_elemental_host(ct.byref(dm.c), ct.byref(a), ne, dg.ptr, bfh.ptr, udg.ptr, uh.ptr, sh.ptr,
+                               o.AE.ptr, o.FE.ptr, o.DUDG.ptr, o.DUDG_DUH.ptr, o.status.ptr, int(bool(mixed)),
+                               int(chunk), _stream_ptr(stream))
+    check(rc, "hdgx_elemental_host")
+    return o
+
+
 def schur_uq(M, C, E, BD, F, GK, H, Rq, Ru, Rh, stream=None):
     """kernel/schur_uq.c: [DUDG, DUDG_DUH, AE, FE] from the reference's elemental blocks."""
     _require_cuda()

@@ -13,6 +13,7 @@
  *
  * Reference call surface each entry point replaces (paths relative to the reference tree):
  *   hdgx_elemental   kernel/hdg_elemental.m:1   [AE,FE,DUDG,DUDG_DUH] = hdg_elemental(master,app,dgnodes,bf,UDG,UH,SH)
+ *   hdgx_elemental_host   kernel/hdg_elemental.m:1   the same call on host arrays (copies overlapped)
  *   hdgx_schur_uq    kernel/schur_uq.c:193      [DUDG,DUDG_DUH,AE,FE] = schur_uq(M,C,E,BD,F,GK,H,Rq,Ru,Rh)
  *   hdgx_schur_u     kernel/schur_u.c:82        [DUDG,DUDG_DUH,AE,FE] = schur_u(BD,F,GK,H,Ru,Rh)
  *   hdgx_globalassembly   kernel/globalassembly.m:1  [Hg,Rg] = globalassembly(mesh,AE,FE)
@@ -94,6 +95,22 @@ int hdgx_elemental_mixed(const hdgx_master *master, const hdgx_app *app, int ne,
                          const double *dgnodes, const int *bf, const double *UDG, const double *UH,
                          const double *SH, double *AE, double *FE, double *DUDG, double *DUDG_DUH,
                          int *status, hdgx_stream_t stream);
+
+/* hdgx_elemental (mixed = 0) or hdgx_elemental_mixed (mixed = 1) on HOST arrays, for callers
+ * whose element data lives in host memory as the reference's does (kernel/hdg_elemental.m:1 is
+ * called with host MATLAB arrays).  master stays a DEVICE table set; dgnodes, bf, UDG, UH, SH,
+ * AE, FE, DUDG, DUDG_DUH and status (may be NULL) are HOST pointers in the layouts of
+ * hdgx_elemental.  Page-locked (pinned) host memory gives full copy bandwidth and overlap;
+ * pageable memory works, with the driver staging its copies.  The elements go through two
+ * device staging sets of `chunk` elements (0: ne / 16, at least 1024) taken from the library's
+ * device pool, and chunk c's upload, chunk c-1's kernel and chunk c-2's download run at the
+ * same time, so the call costs about the largest of the three totals.  The results are
+ * bitwise those of the device-array call.  The call returns when the outputs are in host
+ * memory (it synchronises `stream`). */
+int hdgx_elemental_host(const hdgx_master *master, const hdgx_app *app, int ne,
+                        const double *dgnodes, const int *bf, const double *UDG, const double *UH,
+                        const double *SH, double *AE, double *FE, double *DUDG, double *DUDG_DUH,
+                        int *status, int mixed, int chunk, hdgx_stream_t stream);
 
 /* Batched local (u,q) Schur complement on the reference MEX layouts (kernel/schur_uq.c):
  * M[npv,npv,ne] C[npv,npv,nd,ne] E[npv,ndf,nd,ne] BD[npv,ncu,npv,nc,ne] F[npv,ncu,ncu,ndf,ne]

@@ -99,3 +99,46 @@ def test_curved_elements_match_oracle(oracle, name, kw):
         assert err < TOL, f"curved {name} {k} relerr {err:.3e}"
     err = relerr(out.DUDG.numpy(), ref["DUDG"])
     assert err < max(TOL, 10.0 * ulp_sensitivity(oracle, P)), f"curved {name} DUDG relerr {err:.3e}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mixed", [False, True])
+@pytest.mark.parametrize("chunk", [0, 5, 13, 1000])
+def test_host_array_entry_point_matches_device_call(oracle, mixed, chunk):
+    """hdgx_elemental_host (host arrays streamed through the GPU in chunks, the last one ragged
+    for chunk 5 and 13 on 32 elements; chunk >= ne is one chunk) gives bitwise the outputs of
+    the device-array call, which the oracle pins; a singular element's status comes back too."""
+    from hdg_b200.elemental import hdg_elemental, hdg_elemental_host
+    P = configs.c2(n=4, porder=3)
+    m, a = P.master, P.app
+    UDG = np.array(P.UDG, copy=True)
+    UDG[:, :, 7] = np.nan                                # element 7 reports a failure
+    dev = hdg_elemental(m, a, P.mesh.dgnodes, P.mesh.bf, UDG, P.uh_elem(), P.SH, mixed=mixed)
+    host = hdg_elemental_host(m, a, P.mesh.dgnodes, P.mesh.bf, UDG, P.uh_elem(), P.SH, mixed=mixed, chunk=chunk)
+    assert not host.AE.t.is_cuda
+    for k in ("AE", "FE", "DUDG", "DUDG_DUH", "status"):
+        assert np.array_equal(getattr(host, k).numpy(), getattr(dev, k).numpy(), equal_nan=True), k
+    st = host.status.numpy()
+    assert st[7] != 0 and np.all(np.delete(st, 7) == 0)
+    if not mixed:                                        # the mixed kernel has its own parity tests
+        ref = oracle.hdg_elemental(m, a, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), P.SH)
+        keep = np.delete(np.arange(UDG.shape[-1]), 7)
+        for k in ("AE", "FE", "DUDG_DUH"):
+            assert relerr(getattr(host, k).numpy()[..., keep], ref[k][..., keep]) < TOL, k
+
+
+@pytest.mark.gpu
+def test_host_array_entry_point_rejects_bad_arguments():
+    from hdg_b200._lib import lib
+    from hdg_b200.elemental import DeviceMaster, app_struct
+    import ctypes as ct
+    P = configs.c1(n=2, porder=1)
+    dm, a = DeviceMaster(P.master), app_struct(P.app)
+    buf = np.zeros(64)
+    p = buf.ctypes.data
+    assert lib().hdgx_elemental_host(ct.byref(dm.c), ct.byref(a), 4, p, p, p, p, p, p, p, p, None, None, 0, 0,
+                                     None) == -1
+    assert lib().hdgx_elemental_host(ct.byref(dm.c), ct.byref(a), 4, p, p, p, p, p, p, p, p, p, None, 0, -1,
+                                     None) == -1
+    assert lib().hdgx_elemental_host(ct.byref(dm.c), ct.byref(a), 0, p, p, p, p, p, p, p, p, p, None, 0, 0,
+                                     None) == 0

@@ -97,18 +97,14 @@ struct RowPrefetch {
 #pragma unroll
                 for (int c = 0; c < BS; c++) acc -= lv[d * BS + c] * ov[d][c];
             return acc;
-        }
+        } else {
 #pragma unroll
-        for (int d = 0; d < MAXD; d++) {
-            if (k[d] < 0) break;
-            const double *oj = in + (size_t)BS * j[d];
-            double ov[BS];
+            for (int d = 0; d < MAXD; d++) {
+                if (k[d] < 0) break;
+                const double *oj = in + (size_t)BS * j[d];
+                double ov[BS];
 #pragma unroll
-            for (int c = 0; c < BS; c++) ov[c] = __ldcg(oj + c);
-            if constexpr (PL) {
-#pragma unroll
-                for (int c = 0; c < BS; c++) acc -= lv[d * BS + c] * ov[c];
-            } else {
+                for (int c = 0; c < BS; c++) ov[c] = __ldcg(oj + c);
                 const double *B = Mg + (size_t)BS * BS * k[d] + r;
                 double bv[BS];
 #pragma unroll
@@ -116,8 +112,8 @@ struct RowPrefetch {
 #pragma unroll
                 for (int c = 0; c < BS; c++) acc -= bv[c] * ov[c];
             }
+            return acc;
         }
-        return acc;
     }
 
     // sum_c inv(U_ii)[r, c] t[c]
@@ -273,19 +269,25 @@ static int launch_cluster(int nlev, const int *plan, const double *Mg, const dou
     return 0;
 }
 
-// Large blocks (bs >= 20: 3D, or 2D p = 4) move several MB of matrix per level, more than 8 SMs
-// stream in the time of a level: they run CTAs of 512 threads (fewer passes per level), in a
-// cluster of 16 (a non-portable size) when the device can place one, else of 8.  (3D Euler
-// p = 2, 399,360 faces: 69.5 ms per apply with 8 CTAs of 256, 57.9 ms with 8 of 512, 37.2 ms
-// with 16 of 512.)
+// Large blocks (bs >= 20: 3D, or 2D p = 4) run CTAs of 512 threads (fewer passes per level).
+// When a level moves more matrix than 8 SMs stream in the time of a level (kWideLevelBytes of
+// factors per level on average) the cluster has 16 CTAs (a non-portable size) when the device
+// can place one, else 8.  (3D Euler p = 2, 399,360 faces, 12 MB per level: 69.5 ms per apply
+// with 8 CTAs of 256, 57.9 ms with 8 of 512, 37.2 ms with 16 of 512.)  Small systems stay on 8:
+// a 16-CTA cluster needs 16 free SMs of one GPC, which concurrent solves rarely leave (64 queued
+// serving requests: 32 solves/s with 16-CTA clusters for their bs = 20 systems, 74 with 8).
+constexpr size_t kWideLevelBytes = 4u << 20;
 template <int BS, int MAXD>
-static int launch_level_sweep(int nlev, const int *plan, const double *Mg, const double *x, double *y, double *v,
-                              cudaStream_t st) {
+static int launch_level_sweep(int nlev, long long nnzb, const int *plan, const double *Mg, const double *x, double *y,
+                              double *v, cudaStream_t st) {
     const size_t smem = sizeof(int) * ((size_t)nlev + 1);
     if (smem > 160 * 1024) return 1;                    // very long schedules: per-level launches
     if constexpr (BS >= 20) {
-        const int rc = launch_cluster<BS, MAXD, 16, 512>(nlev, plan, Mg, x, y, v, smem, st);
-        if (rc != 2) return rc;
+        const size_t level_bytes = sizeof(double) * BS * BS * (size_t)nnzb / (size_t)nlev;
+        if (level_bytes >= kWideLevelBytes) {
+            const int rc = launch_cluster<BS, MAXD, 16, 512>(nlev, plan, Mg, x, y, v, smem, st);
+            if (rc != 2) return rc;
+        }
         return launch_cluster<BS, MAXD, 8, 512>(nlev, plan, Mg, x, y, v, smem, st) == 0 ? 0 : 1;
     } else {
         return launch_cluster<BS, MAXD, kSweepCS, kSweepNT>(nlev, plan, Mg, x, y, v, smem, st) == 0 ? 0 : 1;
@@ -300,8 +302,8 @@ int level_sweep_apply(const hdgx_bsr *A, const double *Mg, const double *x, doub
     switch (A->bs) {
 #define HDGX_LS(B)                                                                                \
     case B:                                                                                       \
-        return md == 4 ? launch_level_sweep<B, 4>(A->ncolors, A->sweep_plan, Mg, x, y, v, st)    \
-                       : launch_level_sweep<B, 6>(A->ncolors, A->sweep_plan, Mg, x, y, v, st);
+        return md == 4 ? launch_level_sweep<B, 4>(A->ncolors, A->nnzb, A->sweep_plan, Mg, x, y, v, st)    \
+                       : launch_level_sweep<B, 6>(A->ncolors, A->nnzb, A->sweep_plan, Mg, x, y, v, st);
         HDGX_LS(8) HDGX_LS(12) HDGX_LS(15) HDGX_LS(16) HDGX_LS(20) HDGX_LS(30)
 #undef HDGX_LS
         default: return 1;

@@ -27,7 +27,8 @@ struct ElemParams {
     const double *shapvt, *shapvg, *shapmv, *shapft, *shapfg, *shapmf;
     const int *perm;
     PhysConst pc;
-    double fc_q;
+    double fc_q, fc_u;
+    int tdep;                  // 1: time-dependent source s = SH_u - fc_u u (volint.m:180-221)
     int nbnd;
     int bcm[HDGX_MAX_BND];
     double bcs[HDGX_MAX_BND * 5];
@@ -102,7 +103,8 @@ struct Plan {
     static constexpr int p_Hp = p_Gp + D::NGT * D::NCU * D::NC;   // [NGT, NCU, NCU] jac * dRh-flux/duh
     static constexpr int p_Rh = p_Hp + D::NGT * D::NCU * D::NCU;
     static constexpr int p_dudg = p_Rh + D::NH;
-    static constexpr int p_SDsep = p_dudg + D::NQ;                // SD when it does not fit the scratch
+    static constexpr int p_jv = p_dudg + D::NQ;                   // [NGV] volume jac (time-dependent mass term)
+    static constexpr int p_SDsep = p_jv + D::NGV;                 // SD when it does not fit the scratch
     static constexpr int p_end = p_SDsep + (SD_ALIAS ? 0 : D::NU * D::NU);
     static constexpr int p_SD = SD_ALIAS ? x_start : p_SDsep;
     // column tiles of DUDG_DUH (reuse the scratch)
@@ -200,7 +202,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     double *s_SD = sm + L::p_SD, *s_R = sm + L::p_R;
     double *s_MiC = sm + L::p_MiC, *s_MiE = sm + L::p_MiE, *s_MiRq = sm + L::p_MiRq;
     double *s_Gp = sm + L::p_Gp, *s_Hp = sm + L::p_Hp, *s_Rh = sm + L::p_Rh, *s_M = sm + L::p_M;
-    double *s_dudg = sm + L::p_dudg;
+    double *s_dudg = sm + L::p_dudg, *s_jv = sm + L::p_jv;
     double *x_Xx = sm + L::x_Xx, *x_jac = sm + L::x_jac, *x_nl = sm + L::x_nl, *x_jf = sm + L::x_jf;
     double *x_ug = sm + L::x_ug, *x_fu = sm + L::x_fu, *x_fuh = sm + L::x_fuh;
     double *x_wrk = sm + L::x_wrk, *x_wrl = sm + L::x_wrl, *x_FH = sm + L::x_FH, *x_BH = sm + L::x_BH;
@@ -324,6 +326,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             for (int g = 0; g < NGV; g++) t += t_vg[r + NPV * g] * t_vt[g + NGV * s] * x_jac[g];
             s_M[i] = P.fc_q * t;
         }
+        if (tid < NGV) s_jv[tid] = x_jac[tid];
         for (int i = tid; i < NPV * NPV * ND; i += NT) {
             const int r = i % NPV, s = (i / NPV) % NPV, d = i / (NPV * NPV);
             double t = 0.0;
@@ -538,6 +541,14 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             },
             [&](int ab, int r, int k, double v) {
                 const int a = ab % NCU, b = ab / NCU;
+                if (P.tdep && a == b) {
+                    // time-dependent problems: the source Jacobian -fc_u on the u components
+                    // (volint.m:215-216) enters BD, hence D, as fc_u * sum_g phi_r phi_k w_g jac_g
+                    double mu = 0.0;
+#pragma unroll
+                    for (int g = 0; g < NGV; g++) mu += t_vg[r + NPV * g] * t_vt[g + NGV * k] * s_jv[g];
+                    v += P.fc_u * mu;
+                }
                 s_SD[(r + NPV * a) + NU * (k + NPV * b)] = v;
             });
         };
@@ -568,6 +579,17 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                             w -= x_FHu[gg + NGT * (a + NCU * (NCU + bd))] * x_ZFr[gg + NGT * bd];
                     }
                     v += t_fg[m + NPF * g] * w;
+                }
+            }
+            if (P.tdep) {
+                // s = SH_u - fc_u u at the volume Gauss points, Ru += shapvg(:,:,1) (s jac)
+                // (volint.m:180-221 with dtcoef = 1 and no axisymmetry; volint.m:241,258)
+                const double *__restrict__ g_sh = P.SH + (size_t)e * NPV * NC + NPV * a;
+                for (int g = 0; g < NGV; g++) {
+                    double st = 0.0;
+#pragma unroll
+                    for (int s = 0; s < NPV; s++) st += t_vt[g + NGV * s] * g_sh[s];
+                    v += t_vg[r + NPV * g] * ((st - x_ug[g + NGV * a] * P.fc_u) * s_jv[g]);
                 }
             }
             s_R[i] = v;
@@ -701,9 +723,9 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             }
             if (s_gslot[0]) {
                 // fall back to partial pivoting on the original system
-                if (L::SD_ALIAS) {
-                    force_piv = true;            // the right-hand sides' inputs are overwritten by SD
-                    __syncthreads();
+                if (L::SD_ALIAS || L::INV_ALIAS) {
+                    force_piv = true;            // the right-hand sides' inputs are overwritten (by SD,
+                    __syncthreads();             // or by the FP32 inverse): evaluate the element again
                     goto elem_start;
                 } else {
                     build_rhs();
@@ -879,6 +901,8 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
     p.pc.kap = p.pc.rinv * gam / (pr * (gam - 1.0));
     p.pc.tau = app->param[5];
     p.fc_q = app->fc_q;
+    p.fc_u = app->fc_u;
+    p.tdep = app->tdep;
     p.nbnd = app->nbnd;
     for (int i = 0; i < HDGX_MAX_BND; i++) p.bcm[i] = app->bcm[i];
     for (int i = 0; i < HDGX_MAX_BND * 5; i++) p.bcs[i] = app->bcs[i];

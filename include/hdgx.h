@@ -60,8 +60,9 @@ typedef struct {
     int nd, ncu, nc;        /* nc = ncu*(nd+1) for the (u,q) form */
     int localsolve;         /* 1: (u,q) form (only form the fused kernel supports) */
     int getdqdg;            /* 1: DUDG/DUDG_DUH carry all nc components (reference default) */
-    double fc_q, fc_u;      /* fc_u and tdep are accepted; the steady path uses tdep = 0 */
-    int tdep;
+    double fc_q, fc_u;      /* fc_u: time-derivative coefficient of a DIRK stage (tdep = 1) */
+    int tdep;               /* 1: time-dependent residual of kernel/volint.m:180-221 (dtcoef = 1, no
+                               axisymmetry): source SH_u - fc_u u, Jacobian -fc_u on the u components */
     double param[8];        /* [gam, epslm, Re, Pr, Minf, tau]; Re = +inf gives Euler */
     int nbnd;               /* number of boundary indices (bf = -1..-nbnd) */
     int bcm[HDGX_MAX_BND];  /* fbou type per boundary index: 5 periodic, 6 Dirichlet */

@@ -26,7 +26,8 @@ class _Master(ct.Structure):
 
 class _App(ct.Structure):
     _fields_ = [("nd", ct.c_int), ("ncu", ct.c_int), ("nc", ct.c_int), ("localsolve", ct.c_int),
-                ("fc_q", ct.c_double), ("param", _dp), ("nbnd", ct.c_int), ("bcm", _ip), ("bcs", _dp)]
+                ("fc_q", ct.c_double), ("param", _dp), ("nbnd", ct.c_int), ("bcm", _ip), ("bcs", _dp),
+                ("fc_u", ct.c_double), ("tdep", ct.c_int)]
 
 
 def build():
@@ -65,7 +66,7 @@ def _keep(master, app):
                 F(master.shapvt), F(master.shapvg), F(master.shapmv), F(master.shapft),
                 F(master.shapfg), F(master.shapmf), I(master.perm))
     a = _App(app.nd, app.ncu, app.nc, app.localsolve, app.fc_q, F(app.param), len(app.bcm),
-             I(app.bcm), F(app.bcs))
+             I(app.bcm), F(app.bcs), float(getattr(app, "fc_u", 0.0)), int(getattr(app, "tdep", 0)))
     return m, a, keep
 
 
@@ -359,3 +360,61 @@ def gmres_dense(K, F, f2f, x0=None, restart=20, tol=1e-6, maxit=None):
     it = L.orc_gmres_dense(nb, nf, nbf, _p(_f(K)), f2.ctypes.data_as(_ip), _p(_f(F)), _p(x), int(restart),
                            ct.c_double(tol), int(maxit), ct.byref(flag), _p(rev))
     return x, flag.value, it, rev[:it]
+
+
+def dirkcoeff(q, p):
+    """kernel/hdg_solve_dirk.m (dirkcoeff): Butcher tableau of the (stages q, order p) DIRK
+    scheme as (d = inv(a), c = b inv(a), t)."""
+    s2, s3 = np.sqrt(2.0), np.sqrt(3.0)
+    tab = {
+        (1, 1): ([[1.0]], [1.0], [1.0]),
+        (1, 2): ([[0.5]], [1.0], [0.5]),
+        (2, 2): ([[1 - 0.5 * s2, 0], [0.5 * s2, 1 - 0.5 * s2]], [0.5 * s2, 1 - 0.5 * s2], [1 - 0.5 * s2, 1]),
+        (2, 3): ([[0.5 + 0.5 / s3, 0], [-1 / s3, 0.5 + 0.5 / s3]], [0.5, 0.5], [0.5 + 0.5 / s3, 0.5 - 0.5 / s3]),
+    }
+    if (q, p) == (3, 3):
+        a1 = 0.4358665215
+        t1 = (1 + a1) / 2
+        b1 = -(6 * a1 ** 2 - 16 * a1 + 1) / 4
+        b2 = (6 * a1 ** 2 - 20 * a1 + 5) / 4
+        tab[(3, 3)] = ([[a1, 0, 0], [t1 - a1, a1, 0], [b1, b2, a1]], [b1, b2, a1], [a1, t1, 1])
+    if (q, p) == (3, 4):
+        a1 = 2 * np.cos(np.pi / 18) / s3
+        tab[(3, 4)] = ([[0.5 * (1 + a1), 0, 0], [-0.5 * a1, 0.5 * (1 + a1), 0], [1 + a1, -(1 + 2 * a1), 0.5 * (1 + a1)]],
+                       [1 / (6 * a1 ** 2), 1 - 1 / (3 * a1 ** 2), 1 / (6 * a1 ** 2)],
+                       [0.5 * (1 + a1), 0.5, 0.5 * (1 - a1)])
+    a, b, t = (np.array(x, dtype=np.float64) for x in tab[(q, p)])
+    d = np.linalg.inv(a)
+    return d, b @ d, t
+
+
+def hdg_solve_dirk(P, time, dt, nstage, torder, tol=1e-10, maxiter=16, gmres_tol=1e-10, nthreads=1):
+    """kernel/hdg_solve_dirk.m:1-80 on the CPU, one step from (P.UDG, P.UH): each stage is the
+    oracle hdg_solve of the time-dependent residual (app.tdep = 1, fc_u = d(s,s), fc_q = 1)
+    with the stage source SDG; the stage guess is the step's start state (the reference resets
+    its q part with getq.m, a guess-only difference).  Returns (Un, Hn)."""
+    import copy
+    from types import SimpleNamespace
+    d, c, t = dirkcoeff(nstage, torder)
+    d = d / dt
+    UDG = np.asarray(P.UDG, dtype=np.float64)
+    UH = np.asarray(P.UH, dtype=np.float64)
+    Un = (1 - c.sum()) * UDG
+    Hn = (1 - c.sum()) * UH
+    UDGn, SDG = [], None
+    for s in range(nstage):
+        if s == 0:
+            SDG = d[0, 0] * UDG
+        elif s == 1:
+            SDG = (d[1, 0] + d[1, 1]) * UDG - d[1, 0] * UDGn[0]
+        else:
+            SDG = ((d[2, 0] + d[2, 1] + d[2, 2]) * UDG - (d[2, 0] / d[1, 0]) * ((d[1, 0] + d[1, 1]) * UDG - SDG)
+                   - d[2, 1] * UDGn[1])
+        app = copy.copy(P.app)
+        app.fc_u, app.fc_q, app.tdep = float(d[s, s]), 1.0, 1
+        Q = SimpleNamespace(master=P.master, app=app, mesh=P.mesh, UDG=UDG, UH=UH, SH=SDG)
+        Us, Hs, _, _, _ = hdg_solve(Q, tol=tol, maxiter=maxiter, gmres_tol=gmres_tol, nthreads=nthreads)
+        UDGn.append(Us)
+        Un = Un + c[s] * Us
+        Hn = Hn + c[s] * Hs
+    return Un, Hn

@@ -7,7 +7,9 @@
  *
  * One element at a time, the same operations as the reference's vectorised MATLAB:
  *   volgeom  kernel/volgeom.m:18-61      pg, Jg = dx/dxi, jac = det Jg, Xx = adj(Jg)
- *   volint   kernel/volint.m:25-60,241-263  M, C, Rq, Ru, BD (source = 0, steady: tdep = 0)
+ *   volint   kernel/volint.m:25-60,241-263  M, C, Rq, Ru, BD (flux source = 0); time-dependent
+ *            problems (tdep = 1, volint.m:180-221 with dtcoef = 1, no axisymmetry) add the
+ *            source s = SH_u - fc_u u and its Jacobian -fc_u on the u components
  *   facegeom kernel/facegeom.m:20-52     pg, nlg, jac at face Gauss points
  *   faceint  kernel/faceint.m:29-61,171-360  E, Rq -= E.UH, fhat, fbou, Ru, BD, F, Rh, GK, H
  *   schur    kernel/schur_primal.m:52-150 (schur_uq2): Mi = inv(M), SD = D + B Mi C,
@@ -42,6 +44,8 @@ typedef struct {
     int nbnd;                      /* number of boundary indices */
     const int *bcm;                /* [nbnd] fbou type per boundary index */
     const double *bcs;             /* [nbnd, ncu] column-major */
+    double fc_u;                   /* time-derivative coefficient (tdep = 1) */
+    int tdep;                      /* 1: time-dependent source (volint.m:180-221) */
 } orc_app;
 
 
@@ -264,6 +268,20 @@ static int element_blocks(const orc_master *ms, const orc_app *ap, const double 
                     t += ms->shapvg[IX3(r, g, i + 1, npv, ngv)] * wrk[IX3(g, i, a, ngv, nd)];
             b->Ru[IX2(r, a, npv)] = t;
         }
+    /* time-dependent source (volint.m:180-221): s(g,a) = Stg(g,a) - fc_u u(g,a) with Stg the
+     * u part of SH at the Gauss points; Ru += shapvg(:,:,1) (s jac) (volint.m:241,258) */
+    if (ap->tdep) {
+        for (int a = 0; a < ncu; a++)
+            for (int r = 0; r < npv; r++) {
+                double t = 0.0;
+                for (int g = 0; g < ngv; g++) {
+                    double st = 0.0;
+                    for (int s = 0; s < npv; s++) st += ms->shapvt[IX3(g, s, 0, ngv, npv)] * sh[IX2(s, a, npv)];
+                    t += ms->shapvg[IX3(r, g, 0, npv, ngv)] * ((st - ug[IX2(g, a, ngv)] * ap->fc_u) * jac[g]);
+                }
+                b->Ru[IX2(r, a, npv)] += t;
+            }
+    }
     /* BD[r,a,s,c] = sum_g sum_i shapvg(r,g,i+1) shapvl(s,g) wrl_i(g,a,c) */
     for (int c = 0; c < nc; c++)
         for (int s = 0; s < npv; s++)
@@ -277,6 +295,16 @@ static int element_blocks(const orc_master *ms, const orc_app *ap, const double 
                         t += w * ms->shapvt[IX3(g, s, 0, ngv, npv)];
                     }
                     b->BD[r + (size_t)npv * (a + (size_t)ncu * (s + (size_t)npv * c))] = t;
+                }
+    /* ... and its Jacobian: wrl(1:ngv, a, a) = fc_u jac, so BD[r,a,s,a] += fc_u sum_g phi_r phi_s w_g jac_g */
+    if (ap->tdep)
+        for (int a = 0; a < ncu; a++)
+            for (int s = 0; s < npv; s++)
+                for (int r = 0; r < npv; r++) {
+                    double t = 0.0;
+                    for (int g = 0; g < ngv; g++)
+                        t += ms->shapvg[IX3(r, g, 0, npv, ngv)] * ms->shapvt[IX3(g, s, 0, ngv, npv)] * jac[g];
+                    b->BD[r + (size_t)npv * (a + (size_t)ncu * (s + (size_t)npv * a))] += ap->fc_u * t;
                 }
 
     /* ---- facegeom (facegeom.m:20-52): per face j, ngf points */

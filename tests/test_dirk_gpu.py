@@ -1,0 +1,69 @@
+"""GPU parity of the time-dependent path: the elemental kernel with app.tdep = 1 against the
+oracle (same tolerances as the steady elemental tests: 1e-12 on AE, FE, DUDG_DUH, and the
+oracle's own one-ulp sensitivity bound on DUDG), and one DIRK step (hdg_b200.dirk) against the
+oracle's restatement of kernel/hdg_solve_dirk.m: each stage is a Newton solve to 1e-10, so the
+step's states agree to 1e-8 relative."""
+import copy
+
+import numpy as np
+import pytest
+
+from hdg_b200 import configs
+
+TOL = 1e-12
+
+
+def relerr(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _tdep(P, fc_u, seed=4):
+    app = copy.copy(P.app)
+    app.tdep, app.fc_u = 1, fc_u
+    rng = np.random.default_rng(seed)
+    SH = np.array(P.SH, copy=True)
+    SH[:, :app.ncu, :] = fc_u * P.UDG[:, :app.ncu, :] * (1.0 + 0.1 * rng.standard_normal(SH[:, :app.ncu, :].shape))
+    return app, SH
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw", [("c1", dict(n=4, porder=2)), ("c2", dict(n=4, porder=3)),
+                                     ("c1", dict(n=3, porder=4)), ("c4", dict(n=2, porder=2))])
+def test_time_dependent_elemental_matches_oracle(oracle, name, kw):
+    from hdg_b200.elemental import hdg_elemental
+    P = configs.by_name(name, **kw)
+    m, mesh = P.master, P.mesh
+    app, SH = _tdep(P, 7.3)
+    ref = oracle.hdg_elemental(m, app, mesh.dgnodes, mesh.bf, P.UDG, P.uh_elem(), SH)
+    assert ref["nbad"] == 0
+    out = hdg_elemental(m, app, mesh.dgnodes, mesh.bf, P.UDG, P.uh_elem(), SH)
+    assert int(out.status.numpy().max()) == 0
+    for k in ("AE", "FE", "DUDG_DUH"):
+        err = relerr(getattr(out, k).numpy(), ref[k])
+        assert err < TOL, f"{name} {kw} {k} relerr {err:.3e}"
+    rng = np.random.default_rng(7)
+    jit = lambda x: x * (1.0 + 2.2e-16 * rng.standard_normal(x.shape))
+    ref1 = oracle.hdg_elemental(m, app, jit(mesh.dgnodes), mesh.bf, jit(P.UDG), jit(P.uh_elem()), SH)
+    bound = max(TOL, 10.0 * relerr(ref1["DUDG"], ref["DUDG"]))
+    err = relerr(out.DUDG.numpy(), ref["DUDG"])
+    assert err < bound, f"{name} {kw} DUDG relerr {err:.3e} > {bound:.3e}"
+    # the mixed form carries the same terms: its residual FE stays FP64-accurate
+    mix = hdg_elemental(m, app, mesh.dgnodes, mesh.bf, P.UDG, P.uh_elem(), SH, mixed=True)
+    assert relerr(mix.FE.numpy(), ref["FE"]) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("q,p", [(2, 2), (3, 3)])
+def test_dirk_step_matches_oracle(oracle, q, p):
+    from hdg_b200.dirk import hdg_solve_dirk
+    P = configs.c1(n=4, porder=2)
+    dt = 0.05
+    Un_ref, Hn_ref = oracle.hdg_solve_dirk(P, 0.0, dt, q, p)
+    Un, Hn, reps = hdg_solve_dirk(P.master, P.mesh, P.app, P.UDG, P.UH, 0.0, dt, q, p)
+    assert len(reps) == q
+    for rep in reps:
+        assert rep.residuals[-1] <= 1e-10 * rep.residuals[0]
+    assert relerr(Un, Un_ref) < 1e-8
+    assert relerr(Hn, Hn_ref) < 1e-8
+    # the step moved the state (a time step, not a steady solve)
+    assert relerr(Un, np.asarray(P.UDG)) > 1e-6

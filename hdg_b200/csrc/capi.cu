@@ -10,6 +10,10 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
                      double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed,
                      int grid);
 cudaMemPool_t device_pool();
+int schur_adjoint_launch(int qform, int nd, int npv, int ncu, int nc, int ndf, int ne, const double *M,
+                         const double *C, const double *E, const double *BD, const double *F, const double *GK,
+                         const double *H, const double *Rq, const double *Ru, const double *Rh, double *DUDG,
+                         double *DUDG_DUH, double *AE, double *FE, int *status, cudaStream_t st);
 int schur_launch(int qform, int nd, int npv, int ncu, int nc, int ndf, int ne, const double *M,
                  const double *C, const double *E, const double *BD, const double *F, const double *GK,
                  const double *H, const double *Rq, const double *Ru, const double *Rh, double *DUDG,
@@ -294,6 +298,28 @@ int hdgx_schur_u(int npv, int ncu, int nc, int ndf, int ne, const double *BD, co
     if (!BD || !F || !GK || !H || !Ru || !Rh || !DUDG || !DUDG_DUH || !AE || !FE) return -1;
     return hdgx::schur_launch(0, 1, npv, ncu, nc, ndf, ne, nullptr, nullptr, nullptr, BD, F, GK, H,
                               nullptr, Ru, Rh, DUDG, DUDG_DUH, AE, FE, status, (cudaStream_t)stream);
+}
+
+int hdgx_schur_uq_adjoint(int nd, int npv, int ncu, int ndf, int ne, const double *M, const double *C,
+                          const double *E, const double *BD, const double *F, const double *GK, const double *H,
+                          const double *Rq, const double *Ru, const double *Rh, double *DUDG, double *DUDG_DUH,
+                          double *AE, double *FE, int *status, hdgx_stream_t stream) {
+    if (ne < 0 || nd < 1 || npv < 1 || ncu < 1 || ndf < 1) return -1;
+    if (ne == 0) return 0;
+    if (!M || !C || !E || !BD || !F || !GK || !H || !Rq || !Ru || !Rh || !DUDG || !DUDG_DUH || !AE || !FE)
+        return -1;
+    return hdgx::schur_adjoint_launch(1, nd, npv, ncu, ncu * (nd + 1), ndf, ne, M, C, E, BD, F, GK, H, Rq, Ru,
+                                      Rh, DUDG, DUDG_DUH, AE, FE, status, (cudaStream_t)stream);
+}
+
+int hdgx_schur_u_adjoint(int npv, int ncu, int nc, int ndf, int ne, const double *BD, const double *F,
+                         const double *GK, const double *H, const double *Ru, const double *Rh, double *DUDG,
+                         double *DUDG_DUH, double *AE, double *FE, int *status, hdgx_stream_t stream) {
+    if (ne < 0 || npv < 1 || ncu < 1 || nc < ncu || ndf < 1) return -1;
+    if (ne == 0) return 0;
+    if (!BD || !F || !GK || !H || !Ru || !Rh || !DUDG || !DUDG_DUH || !AE || !FE) return -1;
+    return hdgx::schur_adjoint_launch(0, 1, npv, ncu, nc, ndf, ne, nullptr, nullptr, nullptr, BD, F, GK, H,
+                                      nullptr, Ru, Rh, DUDG, DUDG_DUH, AE, FE, status, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -231,3 +231,38 @@ def schur_u(BD, F, GK, H, Ru, Rh, stream=None):
                         st.ptr, _stream_ptr(stream))
     check(rc, "hdgx_schur_u")
     return DUDG, DD, AE, FE, st
+
+
+def schur_uq_adjoint(M, C, E, BD, F, GK, H, Rq, Ru, Rh, stream=None):
+    """kernel/schur_uq_adjoint.c: the transposed (adjoint) local Schur complement,
+    [DUDG, DUDG_DUH, AE, FE] from the same blocks as ``schur_uq``."""
+    _require_cuda()
+    L = lib()
+    arrs = [as_darray(x) for x in (M, C, E, BD, F, GK, H, Rq, Ru, Rh)]
+    npv, ne = arrs[0].shape[0], arrs[0].shape[-1]
+    ndf, nd = arrs[2].shape[1], arrs[2].shape[2]
+    ncu, nc = arrs[3].shape[1], arrs[3].shape[3]
+    DUDG = DArray.empty((npv, nc, ne)); DD = DArray.empty((npv, nc, ncu, ndf, ne))
+    AE = DArray.empty((ncu, ndf, ncu, ndf, ne)); FE = DArray.empty((ncu, ndf, ne))
+    st = DArray.zeros((ne,), dtype=torch.int32)
+    rc = L.hdgx_schur_uq_adjoint(nd, npv, ncu, ndf, ne, *[x.ptr for x in arrs], DUDG.ptr, DD.ptr, AE.ptr, FE.ptr,
+                                 st.ptr, _stream_ptr(stream))
+    check(rc, "hdgx_schur_uq_adjoint")
+    return DUDG, DD, AE, FE, st
+
+
+def schur_u_adjoint(BD, F, GK, H, Ru, Rh, stream=None):
+    """kernel/schur_u_adjoint.c: the transposed u-only local Schur complement (du and dlu fill
+    the start of each element's DUDG / DUDG_DUH slab, the rest is zero, as that MEX writes)."""
+    _require_cuda()
+    L = lib()
+    arrs = [as_darray(x) for x in (BD, F, GK, H, Ru, Rh)]
+    npv, ncu, nc, ne = arrs[0].shape[0], arrs[0].shape[1], arrs[0].shape[3], arrs[0].shape[-1]
+    ndf = arrs[1].shape[3]
+    DUDG = DArray.empty((npv, nc, ne)); DD = DArray.empty((npv, nc, ncu, ndf, ne))
+    AE = DArray.empty((ncu, ndf, ncu, ndf, ne)); FE = DArray.empty((ncu, ndf, ne))
+    st = DArray.zeros((ne,), dtype=torch.int32)
+    rc = L.hdgx_schur_u_adjoint(npv, ncu, nc, ndf, ne, *[x.ptr for x in arrs], DUDG.ptr, DD.ptr, AE.ptr, FE.ptr,
+                                st.ptr, _stream_ptr(stream))
+    check(rc, "hdgx_schur_u_adjoint")
+    return DUDG, DD, AE, FE, st

@@ -16,6 +16,8 @@
  *   hdgx_elemental_host   kernel/hdg_elemental.m:1   the same call on host arrays (copies overlapped)
  *   hdgx_schur_uq    kernel/schur_uq.c:193      [DUDG,DUDG_DUH,AE,FE] = schur_uq(M,C,E,BD,F,GK,H,Rq,Ru,Rh)
  *   hdgx_schur_u     kernel/schur_u.c:82        [DUDG,DUDG_DUH,AE,FE] = schur_u(BD,F,GK,H,Ru,Rh)
+ *   hdgx_schur_uq_adjoint  kernel/schur_uq_adjoint.c:300  [DUDG,DUDG_DUH,AE,FE] = schur_uq_adjoint(M,C,E,BD,F,GK,H,Rq,Ru,Rh)
+ *   hdgx_schur_u_adjoint   kernel/schur_u_adjoint.c:145   [DUDG,DUDG_DUH,AE,FE] = schur_u_adjoint(BD,F,GK,H,Ru,Rh)
  *   hdgx_globalassembly   kernel/globalassembly.m:1  [Hg,Rg] = globalassembly(mesh,AE,FE)
  *   hdgx_matvec           kernel/matvec.m:1          Xg = matvec(mesh,Hg,Rg)
  *   hdgx_bilu0_factor     kernel/computeBILU0.m:1    Mg = computeBILU0(mesh,Hg)
@@ -154,6 +156,23 @@ int hdgx_schur_u(int npv, int ncu, int nc, int ndf, int ne,
                  const double *BD, const double *F, const double *GK, const double *H,
                  const double *Ru, const double *Rh, double *DUDG, double *DUDG_DUH,
                  double *AE, double *FE, int *status, hdgx_stream_t stream);
+
+/* Adjoint (transposed) local Schur complements, the reference's schur_uq_adjoint.c and
+ * schur_u_adjoint.c on the same layouts and arguments as hdgx_schur_uq / hdgx_schur_u: the
+ * local system is solved with D^T (plus, for the (u,q) form, the transposed B Mi C coupling),
+ * the trace coupling uses GK^T, F^T and H^T.  The u form writes, as that MEX does, du into the
+ * first npv*ncu entries of each element's DUDG slab and dlu (column-major [npv*ncu, ncu*ndf])
+ * into the first npv*ncu*ncu*ndf entries of its DUDG_DUH slab, and zeros elsewhere.  Inputs are
+ * not modified (the reference MEX overwrites M, Rq and Ru).  status as hdgx_schur_uq. */
+int hdgx_schur_uq_adjoint(int nd, int npv, int ncu, int ndf, int ne,
+                          const double *M, const double *C, const double *E, const double *BD,
+                          const double *F, const double *GK, const double *H, const double *Rq,
+                          const double *Ru, const double *Rh, double *DUDG, double *DUDG_DUH,
+                          double *AE, double *FE, int *status, hdgx_stream_t stream);
+int hdgx_schur_u_adjoint(int npv, int ncu, int nc, int ndf, int ne,
+                         const double *BD, const double *F, const double *GK, const double *H,
+                         const double *Ru, const double *Rh, double *DUDG, double *DUDG_DUH,
+                         double *AE, double *FE, int *status, hdgx_stream_t stream);
 
 /* ---------------------------------------------------------------- trace system */
 

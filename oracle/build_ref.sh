@@ -1,8 +1,9 @@
 #!/usr/bin/env bash
 # Compile the reference's own C sources for this path, where they lie in the reference
 # tree, into oracle/_ref/ (git-ignored; travels with the snapshot).  Test infrastructure:
-#   schur_uq.so / schur_u.so / arraymul.so : kernel/schur_uq.c, kernel/schur_u.c,
-#       kernel/arraymul.c + the MEX emulation in oracle/refshim, against numpy's ILP64
+#   schur_uq.so / schur_u.so / arraymul.so / schur_uq_adjoint.so / schur_u_adjoint.so :
+#       kernel/schur_uq.c, kernel/schur_u.c, kernel/arraymul.c, kernel/schur_uq_adjoint.c,
+#       kernel/schur_u_adjoint.c + the MEX emulation in oracle/refshim, against numpy's ILP64
 #       OpenBLAS (MATLAB's BLAS ABI uses ptrdiff_t integers);
 #   libref_ns.so : application/FM/ns/{flux,fhat}_ns{2,3}d.c and
 #       application/FM/euler/{flux,fhat}_euler{2,3}d.c (generated point kernels).
@@ -15,7 +16,7 @@ OUT="$HERE/_ref"
 mkdir -p "$OUT"
 OB=$(python -c 'import numpy, glob, os; print(glob.glob(os.path.join(os.path.dirname(numpy.__file__), os.pardir, "numpy.libs", "libscipy_openblas64_*.so"))[0])')
 OBDIR=$(dirname "$OB"); OBNAME=$(basename "$OB")
-for f in schur_uq schur_u arraymul; do
+for f in schur_uq schur_u arraymul schur_uq_adjoint schur_u_adjoint; do
   gcc -O2 -fPIC -shared -w -I"$HERE/refshim" -o "$OUT/$f.so" "$REF/kernel/$f.c" "$HERE/refshim/mexharness.c" \
       "$OB" -Wl,-rpath,"$OBDIR" -lm
 done

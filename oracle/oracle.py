@@ -418,3 +418,71 @@ def hdg_solve_dirk(P, time, dt, nstage, torder, tol=1e-10, maxiter=16, gmres_tol
         Un = Un + c[s] * Us
         Hn = Hn + c[s] * Hs
     return Un, Hn
+
+
+def schur_uq_adjoint(M, C, E, BD, F, GK, H, Rq, Ru, Rh):
+    """kernel/schur_uq_adjoint.c (localsolveuq :43-298) restated with numpy, per element:
+    SDt = D^T + sum_n C_n^T Mi B_n^T, [du, dlu] = SDt \\ [Ru + sum_n C_n^T Mi Rq_n,
+    -(K^T + sum_n C_n^T Mi G_n^T)], dq_n = Mi (Rq_n - B_n^T du), dlq_n = -Mi (B_n^T dlu + G_n^T),
+    FE = Rh - F^T du - sum_n E_n^T dq_n, AE = H^T + F^T dlu + sum_n E_n^T dlq_n
+    (Mi, C_n^T, E_n^T act on the node index of every component)."""
+    npv, ncu, _, nc, ne = BD.shape
+    nd = C.shape[2]; ndf = E.shape[1]; nu, nh = npv * ncu, ncu * ndf
+    DUDG = np.zeros((npv, nc, ne), order="F"); DD = np.zeros((npv, nc, ncu, ndf, ne), order="F")
+    AE = np.zeros((ncu, ndf, ncu, ndf, ne), order="F"); FE = np.zeros((ncu, ndf, ne), order="F")
+    mat = lambda a, r, c: a.reshape((r, c), order="F")
+    for e in range(ne):
+        Mi = np.linalg.inv(M[:, :, e])
+        node = lambda A, X: np.einsum("st,tb...->sb...", A, X)      # act on the node index
+        D = mat(BD[:, :, :, :ncu, e], nu, nu)
+        K = mat(GK[:, :, :, :ncu, e], nh, nu)
+        SDt = D.T.copy()
+        R0 = Ru[:, :, e].copy()
+        KT = K.T.reshape((npv, ncu, nh), order="F").copy()
+        Bn = [mat(BD[:, :, :, ncu + ncu * n:2 * ncu + ncu * n, e], nu, nu) for n in range(nd)]
+        Gn = [mat(GK[:, :, :, ncu + ncu * n:2 * ncu + ncu * n, e], nh, nu) for n in range(nd)]
+        for n in range(nd):
+            W = C[:, :, n, e].T @ Mi
+            SDt += mat(node(W, Bn[n].T.reshape((npv, ncu, nu), order="F")), nu, nu)
+            R0 += W @ Rq[:, :, n, e]
+            KT += node(W, Gn[n].T.reshape((npv, ncu, nh), order="F"))
+        X = np.linalg.solve(SDt, np.column_stack([R0.ravel(order="F"), -mat(KT, nu, nh)]))
+        du, dlu = X[:, 0], X[:, 1:]
+        dq = [node(Mi, Rq[:, :, n, e] - (Bn[n].T @ du).reshape((npv, ncu), order="F")) for n in range(nd)]
+        dlq = [-node(Mi, (Bn[n].T @ dlu + Gn[n].T).reshape((npv, ncu, nh), order="F")) for n in range(nd)]
+        DUDG[:, :ncu, e] = du.reshape((npv, ncu), order="F")
+        DD[:, :ncu, :, :, e] = dlu.reshape((npv, ncu, ncu, ndf), order="F")
+        for n in range(nd):
+            DUDG[:, ncu + ncu * n:2 * ncu + ncu * n, e] = dq[n]
+            DD[:, ncu + ncu * n:2 * ncu + ncu * n, :, :, e] = dlq[n].reshape((npv, ncu, ncu, ndf), order="F")
+        Ft = mat(F[:, :, :, :, e], nu, nh).T
+        fe = Rh[:, :, e].ravel(order="F") - Ft @ du
+        ae = mat(H[:, :, :, :, e], nh, nh).T + Ft @ dlu
+        for n in range(nd):
+            En = E[:, :, n, e]                                          # [npv, ndf]
+            fe -= (En.T @ dq[n]).T.ravel(order="F")                     # (a, f) <- sum_s E(s,f) dq(s,a)
+            ae += np.einsum("sf,sak->afk", En, dlq[n]).reshape((nh, nh), order="F")
+        FE[:, :, e] = fe.reshape((ncu, ndf), order="F")
+        AE[:, :, :, :, e] = ae.reshape((ncu, ndf, ncu, ndf), order="F")
+    return DUDG, DD, AE, FE
+
+
+def schur_u_adjoint(BD, F, GK, H, Ru, Rh):
+    """kernel/schur_u_adjoint.c (localsolve :43-143) restated with numpy: [du, dlu] = D^T \\
+    [Ru, -K^T], FE = Rh - F^T du, AE = H^T + F^T dlu; du and dlu (column-major) fill the start of
+    each element's DUDG / DUDG_DUH slab, the rest zero, as that MEX writes them."""
+    npv, ncu, _, nc, ne = BD.shape
+    ndf = H.shape[1]; nu, nh = npv * ncu, ncu * ndf
+    DUDG = np.zeros((npv * nc, ne)); DD = np.zeros((npv * nc * nh, ne))
+    AE = np.zeros((nh * nh, ne)); FE = np.zeros((nh, ne))
+    for e in range(ne):
+        D = BD[:, :, :, :ncu, e].reshape((nu, nu), order="F")
+        K = GK[:, :, :, :ncu, e].reshape((nh, nu), order="F")
+        X = np.linalg.solve(D.T, np.column_stack([Ru[:, :, e].ravel(order="F"), -K.T]))
+        Ft = F[:, :, :, :, e].reshape((nu, nh), order="F").T
+        DUDG[:nu, e] = X[:, 0]
+        DD[:nu * nh, e] = X[:, 1:].ravel(order="F")
+        FE[:, e] = Rh[:, :, e].ravel(order="F") - Ft @ X[:, 0]
+        AE[:, e] = (H[:, :, :, :, e].reshape((nh, nh), order="F").T + Ft @ X[:, 1:]).ravel(order="F")
+    return (DUDG.reshape((npv, nc, ne), order="F"), DD.reshape((npv, nc, ncu, ndf, ne), order="F"),
+            AE.reshape((ncu, ndf, ncu, ndf, ne), order="F"), FE.reshape((ncu, ndf, ne), order="F"))

@@ -9,8 +9,11 @@
                         kernel/schur_u.c (compiled into oracle/_ref with the MEX emulation)
                         on the elemental blocks of a 2D Euler p=2 case (8 elements) and a
                         2D Navier-Stokes p=3 case (8 elements).
+* ref_schur_adjoint.npz -- outputs of kernel/schur_uq_adjoint.c and kernel/schur_u_adjoint.c
+                        (compiled the same way) on the blocks stored in ref_schur.npz; the u
+                        form both on the D block alone and on the full BD / GK (nc > ncu).
 
-Usage: python tests/golden/make_golden.py [reference-root]
+Usage: python tests/golden/make_golden.py [reference-root] [--only adjoint]
 """
 import sys
 from pathlib import Path
@@ -32,6 +35,27 @@ def _master(struct):
         if k in struct.dtype.names:
             out[k] = np.array(struct[k], dtype=np.float64)
     return out
+
+
+def adjoint_fixture():
+    from oracle import oracle as O
+    d = np.load(OUT / "ref_schur.npz")
+    adj = {}
+    for tag in ("euler2d", "ns2d"):
+        g = lambda k: np.array(d[f"{tag}_{k}"])
+        npv, ncu, _, nc, ne = g("BD").shape
+        ndf = g("H").shape[1]
+        outs = O.ref_mex("schur_uq_adjoint.so", [g(k) for k in ("M", "C", "E", "BD", "F", "GK", "H", "Rq", "Ru", "Rh")],
+                         [(npv, nc, ne), (npv, nc, ncu, ndf, ne), (ncu, ndf, ncu, ndf, ne), (ncu, ndf, ne)])
+        for k, v in zip(("DUDG", "DUDG_DUH", "AE", "FE"), outs):
+            adj[f"{tag}_uqadj_{k}"] = v
+        for form, BD, GK in (("uadj", g("BDu"), g("GKu")), ("uadjfull", g("BD"), g("GK"))):
+            ncx = BD.shape[3]
+            outs = O.ref_mex("schur_u_adjoint.so", [BD, g("F"), GK, g("H"), g("Ru"), g("Rh")],
+                             [(npv, ncx, ne), (npv, ncx, ncu, ndf, ne), (ncu, ndf, ncu, ndf, ne), (ncu, ndf, ne)])
+            for k, v in zip(("DUDG", "DUDG_DUH", "AE", "FE"), outs):
+                adj[f"{tag}_{form}_{k}"] = v
+    np.savez_compressed(OUT / "ref_schur_adjoint.npz", **adj)
 
 
 def main(ref):
@@ -85,9 +109,15 @@ def main(ref):
         for k, v in zip(("DUDG", "DUDG_DUH", "AE", "FE"), outs):
             sch[f"{tag}_u_{k}"] = v
     np.savez_compressed(OUT / "ref_schur.npz", **sch)
+    adjoint_fixture()
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [x for x in sys.argv[1:] if not x.startswith("--only")]
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1:][:1] == ["adjoint"]:
+        args = [x for x in args if x != "adjoint"]
+        adjoint_fixture()
+    else:
+        main(args[0] if args else "/root/reference")

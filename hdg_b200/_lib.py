@@ -101,6 +101,8 @@ def _declare(L):
     L.hdgx_elemental_host.argtypes = [p(HdgxMaster), p(HdgxApp), i] + [v] * 10 + [i, i, v]
     L.hdgx_schur_uq.restype = i
     L.hdgx_schur_uq.argtypes = [i] * 5 + [v] * 15 + [v]
+    L.hdgx_getq.restype = i
+    L.hdgx_getq.argtypes = [p(HdgxMaster), p(HdgxApp), i] + [v] * 7 + [v]
     L.hdgx_schur_uq_adjoint.restype = i
     L.hdgx_schur_uq_adjoint.argtypes = [i] * 5 + [v] * 15 + [v]
     L.hdgx_schur_u_adjoint.restype = i

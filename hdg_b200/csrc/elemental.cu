@@ -37,6 +37,7 @@ struct ElemParams {
     const int *bf;
     double *AE, *FE, *DUDG, *DUDG_DUH;
     int *status;
+    double *QDG;               // non-NULL: getq mode (kernel/getq.m), the element stops after inv(M)
 };
 
 template <int ND_, int NPV_, int NPF_, int NGV_, int NGF_>
@@ -361,7 +362,8 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             double t = 0.0;
 #pragma unroll
             for (int s = 0; s < NPV; s++)
-                t += s_M[r + NPV * s] * (g_shq[s + NPV * (a + NCU * d)] / P.fc_q - s_udg[s + NPV * cq]);
+                t += s_M[r + NPV * s] * ((P.SH ? g_shq[s + NPV * (a + NCU * d)] / P.fc_q : 0.0) -
+                                         (P.QDG ? 0.0 : s_udg[s + NPV * cq]));   // getq: q does not enter
 #pragma unroll
             for (int s = 0; s < NPV; s++) t += s_MiC[r + NPV * (s + NPV * d)] * s_udg[s + NPV * a];
             for (int f = 0; f < NDF; f++) t -= s_MiE[r + NPV * (f + NDF * d)] * s_uh[a + NCU * f];
@@ -374,6 +376,15 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         gj_regs_nopiv<NPV, NPV * ND + NDF * ND + NCU * ND, NT, 8>(s_M, s_MiC, s_pcol, s_bad);
         if (tid == 0 && *s_bad) *s_bad = 1;
         __syncthreads();
+        if (P.QDG) {
+            // getq.m:37-104: the q that zeroes Rq for this u and uh; with q left out of Rq above,
+            // Mi Rq = inv(fc_q Mu) (fc_q Mu SH_q / fc_q + C u - E uh)
+            double *g_q = P.QDG + (size_t)e * NPV * NCU * ND;
+            for (int i = tid; i < NPV * NCU * ND; i += NT) g_q[i] = s_MiRq[i];
+            if (tid == 0 && P.status) P.status[e] = *s_bad;
+            __syncthreads();
+            continue;
+        }
 
         // ================================ flux / fhat / fbou at the Gauss points
         // volume: thread (g, seed); volint.m:81, 241-254
@@ -584,11 +595,11 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             if (P.tdep) {
                 // s = SH_u - fc_u u at the volume Gauss points, Ru += shapvg(:,:,1) (s jac)
                 // (volint.m:180-221 with dtcoef = 1 and no axisymmetry; volint.m:241,258)
-                const double *__restrict__ g_sh = P.SH + (size_t)e * NPV * NC + NPV * a;
+                const double *__restrict__ g_sh = P.SH ? P.SH + (size_t)e * NPV * NC + NPV * a : nullptr;
                 for (int g = 0; g < NGV; g++) {
                     double st = 0.0;
 #pragma unroll
-                    for (int s = 0; s < NPV; s++) st += t_vt[g + NGV * s] * g_sh[s];
+                    for (int s = 0; s < NPV; s++) st += t_vt[g + NGV * s] * (g_sh ? g_sh[s] : 0.0);
                     v += t_vg[r + NPV * g] * ((st - x_ug[g + NGV * a] * P.fc_u) * s_jv[g]);
                 }
             }
@@ -891,7 +902,7 @@ static int launch_v(const ElemParams &p, bool visc, bool mixed, cudaStream_t st,
 int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const double *dgnodes,
                      const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
                      double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed,
-                     int grid) {
+                     int grid, double *QDG) {
     ElemParams p;
     p.shapvt = m->shapvt; p.shapvg = m->shapvg; p.shapmv = m->shapmv;
     p.shapft = m->shapft; p.shapfg = m->shapfg; p.shapmf = m->shapmf; p.perm = m->perm;
@@ -908,6 +919,7 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
     for (int i = 0; i < HDGX_MAX_BND * 5; i++) p.bcs[i] = app->bcs[i];
     p.ne = ne; p.dgnodes = dgnodes; p.UDG = UDG; p.UH = UH; p.SH = SH; p.bf = bf;
     p.AE = AE; p.FE = FE; p.DUDG = DUDG; p.DUDG_DUH = DUDG_DUH; p.status = status;
+    p.QDG = QDG;
     const bool visc = p.pc.rinv != 0.0;
     const int nd = m->nd, po = m->porder;
     if (nd == 2) {

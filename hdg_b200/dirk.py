@@ -6,12 +6,10 @@ source ``SH_u - fc_u u`` and its Jacobian ``-fc_u`` on the u components (``app.t
 with ``fc_u = d(s, s)`` and the stage source ``SH`` built from the step's start state and the
 earlier stages' solutions as hdg_solve_dirk.m builds SDG.
 
-Differences from the reference driver, both on the stage's initial guess only:
-* hdg_solve_dirk.m resets the q components of the guess with getq.m before every stage
-  (written for a 3-component model: ``UDG(:,4:9,:)``); here the guess is the step's start state
-  with its own q.  Newton solves for (u, q, uh) together, so the stage solution is the same to
-  the Newton tolerance.
-* ``app.wave`` (fc_q = fc_u and the PDG auxiliary variable) is not supported.
+As the reference does, every stage first forms its source SDG from the current UDG and then
+resets the q components of UDG with getq.m (``hdgx_getq`` on the GPU); the reference writes
+them as ``UDG(:,4:9,:)``, i.e. for a 3-component model, here they are the components
+``ncu+1:nc``.  ``app.wave`` (fc_q = fc_u and the PDG auxiliary variable) is not supported.
 """
 from __future__ import annotations
 
@@ -20,6 +18,8 @@ import math
 
 import numpy as np
 
+from .app import gather_uh
+from .elemental import getq
 from .solve import hdg_solve
 
 
@@ -83,11 +83,16 @@ def hdg_solve_dirk(master, mesh, app, UDG, UH, time, dt, nstage, torder, tol=1e-
     Un = (1.0 - c.sum()) * UDG
     Hn = (1.0 - c.sum()) * UH
     sols, reports, SDG = [], [], None
+    ncu = app.ncu
+    UHe = gather_uh(UH, mesh.elcon)
     for s in range(nstage):
         SDG = stage_source(d, s, UDG, sols, SDG)
         sapp = copy.copy(app)
         sapp.fc_u, sapp.fc_q, sapp.tdep = float(d[s, s]), 1.0, 1
         sapp.time = time + dt * t[s]
+        Q, _ = getq(master, sapp, mesh.dgnodes, mesh.bf, UDG, UHe, None, sapp.fc_q)
+        UDG = np.array(UDG, copy=True)
+        UDG[:, ncu:, :] = Q.numpy()
         Us, Hs, rep = hdg_solve(master, mesh, sapp, UDG, UH, SDG, tol=tol, maxiter=maxiter, gmres_tol=gmres_tol,
                                 restart=restart, ordering=ordering, mixed=mixed)
         sols.append(Us)

@@ -154,6 +154,30 @@ def hdg_elemental(master, app, dgnodes, bf, UDG, UH, SH, out=None, stream=None, 
     return o
 
 
+def getq(master, app, dgnodes, bf, UDG, UH, SH=None, fc_q=None, stream=None, dmaster=None):
+    """kernel/getq.m: QDG[npv, ncu*nd, ne], the q that zeroes the local q equation for the
+    given u and element-gathered trace UH (``SH`` None: no source, as getq(...,[],fc_q));
+    ``fc_q`` defaults to ``app.fc_q``.  Returns (QDG, status) as DArrays."""
+    import copy
+    _require_cuda()
+    L = lib()
+    dm = dmaster if dmaster is not None else DeviceMaster(master)
+    if fc_q is not None:
+        app = copy.copy(app)
+        app.fc_q = float(fc_q)
+    dg, udg, uh = (as_darray(x) for x in (dgnodes, UDG, UH))
+    sh = as_darray(SH) if SH is not None else None
+    bfd = as_darray(bf, dtype=torch.int32)
+    ne = udg.shape[-1]
+    Q = DArray.empty((master.npv, app.ncu * master.nd, ne))
+    st = DArray.zeros((ne,), dtype=torch.int32)
+    a = app_struct(app)
+    rc = L.hdgx_getq(ct.byref(dm.c), ct.byref(a), ne, dg.ptr, bfd.ptr, udg.ptr, uh.ptr, sh.ptr if sh else None,
+                     Q.ptr, st.ptr, _stream_ptr(stream))
+    check(rc, "hdgx_getq")
+    return Q, st
+
+
 def as_host_darray(x, dtype=torch.float64):
     """A column-major page-locked host DArray of ``x`` (a numpy array, or a host DArray kept as is)."""
     if isinstance(x, DArray):

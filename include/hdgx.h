@@ -16,6 +16,7 @@
  *   hdgx_elemental_host   kernel/hdg_elemental.m:1   the same call on host arrays (copies overlapped)
  *   hdgx_schur_uq    kernel/schur_uq.c:193      [DUDG,DUDG_DUH,AE,FE] = schur_uq(M,C,E,BD,F,GK,H,Rq,Ru,Rh)
  *   hdgx_schur_u     kernel/schur_u.c:82        [DUDG,DUDG_DUH,AE,FE] = schur_u(BD,F,GK,H,Ru,Rh)
+ *   hdgx_getq        kernel/getq.m:1            QDG = getq(master,mesh,UDG,UH,SH,fc_q)
  *   hdgx_schur_uq_adjoint  kernel/schur_uq_adjoint.c:300  [DUDG,DUDG_DUH,AE,FE] = schur_uq_adjoint(M,C,E,BD,F,GK,H,Rq,Ru,Rh)
  *   hdgx_schur_u_adjoint   kernel/schur_u_adjoint.c:145   [DUDG,DUDG_DUH,AE,FE] = schur_u_adjoint(BD,F,GK,H,Ru,Rh)
  *   hdgx_globalassembly   kernel/globalassembly.m:1  [Hg,Rg] = globalassembly(mesh,AE,FE)
@@ -156,6 +157,15 @@ int hdgx_schur_u(int npv, int ncu, int nc, int ndf, int ne,
                  const double *BD, const double *F, const double *GK, const double *H,
                  const double *Ru, const double *Rh, double *DUDG, double *DUDG_DUH,
                  double *AE, double *FE, int *status, hdgx_stream_t stream);
+
+/* getq.m: the gradient unknowns q that zero the local q equation for the given u and trace,
+ * QDG = SH_q/fc_q + inv(fc_q M) (C u - E uh) per element (volint.m:57-60 / faceint.m:49-51 with
+ * Rq = 0), computed by the first phases of the elemental kernel.  Arguments as hdgx_elemental
+ * (UH element-gathered; app supplies nd, ncu, nc, fc_q != 0); SH may be NULL (no source, as
+ * getq(...,[],fc_q)); QDG[npv, ncu*nd, ne]; status 1 for a singular mass matrix. */
+int hdgx_getq(const hdgx_master *master, const hdgx_app *app, int ne, const double *dgnodes,
+              const int *bf, const double *UDG, const double *UH, const double *SH, double *QDG,
+              int *status, hdgx_stream_t stream);
 
 /* Adjoint (transposed) local Schur complements, the reference's schur_uq_adjoint.c and
  * schur_u_adjoint.c on the same layouts and arguments as hdgx_schur_uq / hdgx_schur_u: the

@@ -389,10 +389,10 @@ def dirkcoeff(q, p):
 
 
 def hdg_solve_dirk(P, time, dt, nstage, torder, tol=1e-10, maxiter=16, gmres_tol=1e-10, nthreads=1):
-    """kernel/hdg_solve_dirk.m:1-80 on the CPU, one step from (P.UDG, P.UH): each stage is the
-    oracle hdg_solve of the time-dependent residual (app.tdep = 1, fc_u = d(s,s), fc_q = 1)
-    with the stage source SDG; the stage guess is the step's start state (the reference resets
-    its q part with getq.m, a guess-only difference).  Returns (Un, Hn)."""
+    """kernel/hdg_solve_dirk.m:1-80 on the CPU, one step from (P.UDG, P.UH): each stage forms
+    its source SDG, resets the q part of UDG with getq (components ncu+1:nc), and is the oracle
+    hdg_solve of the time-dependent residual (app.tdep = 1, fc_u = d(s,s), fc_q = 1).
+    Returns (Un, Hn)."""
     import copy
     from types import SimpleNamespace
     d, c, t = dirkcoeff(nstage, torder)
@@ -412,6 +412,10 @@ def hdg_solve_dirk(P, time, dt, nstage, torder, tol=1e-10, maxiter=16, gmres_tol
                    - d[2, 1] * UDGn[1])
         app = copy.copy(P.app)
         app.fc_u, app.fc_q, app.tdep = float(d[s, s]), 1.0, 1
+        from hdg_b200.app import gather_uh
+        UDG = np.array(UDG, copy=True)
+        UDG[:, app.ncu:, :] = getq(P.master, app, P.mesh.dgnodes, P.mesh.bf, UDG, gather_uh(UH, P.mesh.elcon),
+                                   None, app.fc_q)
         Q = SimpleNamespace(master=P.master, app=app, mesh=P.mesh, UDG=UDG, UH=UH, SH=SDG)
         Us, Hs, _, _, _ = hdg_solve(Q, tol=tol, maxiter=maxiter, gmres_tol=gmres_tol, nthreads=nthreads)
         UDGn.append(Us)
@@ -486,3 +490,26 @@ def schur_u_adjoint(BD, F, GK, H, Ru, Rh):
         AE[:, e] = (H[:, :, :, :, e].reshape((nh, nh), order="F").T + Ft @ X[:, 1:]).ravel(order="F")
     return (DUDG.reshape((npv, nc, ne), order="F"), DD.reshape((npv, nc, ncu, ndf, ne), order="F"),
             AE.reshape((ncu, ndf, ncu, ndf, ne), order="F"), FE.reshape((ncu, ndf, ne), order="F"))
+
+
+def getq(master, app, dgnodes, bf, UDG, UHe, SH=None, fc_q=1.0):
+    """kernel/getq.m on the CPU: QDG[npv, ncu*nd, ne] = inv(fc_q Mu) (C u - E uh) + SH_q/fc_q, with
+    Mu, C, E the oracle's volint/faceint blocks (getq.m's local volgeom negates both the adjugate
+    and the face normal, so its Mi (E uh - C u) is this same expression)."""
+    import copy
+    a = copy.copy(app)
+    a.fc_q = float(fc_q)
+    a.tdep = 0
+    ne = UDG.shape[-1]
+    ncu, nd, npv = a.ncu, master.nd, master.npv
+    zero = np.zeros_like(UDG)
+    blk = hdg_elemental(master, a, dgnodes, bf, UDG, UHe, zero, intermediates=True)
+    Q = np.zeros((npv, ncu * nd, ne), order="F")
+    for e in range(ne):
+        Mi = np.linalg.inv(blk["M"][:, :, e])
+        for d in range(nd):
+            rhs = blk["C"][:, :, d, e] @ UDG[:, :ncu, e] - blk["E"][:, :, d, e] @ UHe[:, :, e].T
+            Q[:, ncu * d:ncu * (d + 1), e] = Mi @ rhs
+    if SH is not None:
+        Q = Q + np.asarray(SH)[:, ncu:, :] / fc_q
+    return Q

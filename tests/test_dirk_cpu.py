@@ -92,3 +92,46 @@ def test_dirk_rejects_unknown_schemes():
     from hdg_b200.dirk import dirk_coefficients
     with pytest.raises(ValueError):
         dirk_coefficients(4, 4)
+
+
+def _linear_state(P, seed=2):
+    """u = a + b x + c y (+ d z) per component, its trace at the face nodes, and -grad u."""
+    m, mesh = P.master, P.mesh
+    ncu, nd = P.app.ncu, m.nd
+    rng = np.random.default_rng(seed)
+    coef = rng.standard_normal((nd + 1, ncu))
+    x = mesh.dgnodes[:, :nd, :]                                   # [npv, nd, ne]
+    UDG = np.zeros_like(P.UDG)
+    UDG[:, :ncu, :] = coef[0][None, :, None] + np.einsum("pde,dc->pce", x, coef[1:])
+    perm = np.asarray(m.perm) - 1                                 # [npf, nfe] 0-based
+    UHe = np.stack([UDG[perm[:, j], :ncu, :] for j in range(perm.shape[1])], axis=0)   # [nfe, npf, ncu, ne]
+    UHe = np.ascontiguousarray(UHe.transpose(2, 1, 0, 3)).reshape((ncu, -1, UDG.shape[-1]), order="F")
+    grad = np.zeros((m.npv, ncu * nd, UDG.shape[-1]))
+    for d in range(nd):
+        grad[:, ncu * d:ncu * (d + 1), :] = coef[1 + d][None, :, None]
+    return UDG, UHe, grad
+
+
+@pytest.mark.parametrize("name,kw", [("c1", dict(n=3, porder=2)), ("c4", dict(n=1, porder=2))])
+def test_oracle_getq_recovers_minus_the_gradient_of_a_linear_field(oracle, name, kw):
+    """getq.m solves M q = C u - E uh; with uh the trace of a linear u this is -grad u exactly."""
+    P = configs.by_name(name, **kw)
+    UDG, UHe, grad = _linear_state(P)
+    Q = oracle.getq(P.master, P.app, P.mesh.dgnodes, P.mesh.bf, UDG, UHe)
+    assert rel(Q, -grad) < 1e-11          # an identity up to the round-off of inv(M) (3D: 3e-12)
+
+
+def test_oracle_getq_zeroes_the_q_equation(oracle):
+    P = configs.c2(n=3, porder=3)
+    rng = np.random.default_rng(9)
+    SH = np.zeros_like(P.UDG)
+    SH[:, P.app.ncu:, :] = rng.standard_normal(SH[:, P.app.ncu:, :].shape)
+    fc_q = 0.7
+    Q = oracle.getq(P.master, P.app, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), SH, fc_q)
+    U = np.array(P.UDG, copy=True)
+    U[:, P.app.ncu:, :] = Q
+    a = copy.copy(P.app)
+    a.fc_q = fc_q
+    blk = oracle.hdg_elemental(P.master, a, P.mesh.dgnodes, P.mesh.bf, U, P.uh_elem(), SH, intermediates=True)
+    scale = np.abs(blk["C"]).max() * np.abs(U).max()
+    assert np.abs(blk["Rq"]).max() < 1e-12 * scale

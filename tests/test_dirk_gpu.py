@@ -1,8 +1,9 @@
 """GPU parity of the time-dependent path: the elemental kernel with app.tdep = 1 against the
 oracle (same tolerances as the steady elemental tests: 1e-12 on AE, FE, DUDG_DUH, and the
-oracle's own one-ulp sensitivity bound on DUDG), and one DIRK step (hdg_b200.dirk) against the
-oracle's restatement of kernel/hdg_solve_dirk.m: each stage is a Newton solve to 1e-10, so the
-step's states agree to 1e-8 relative."""
+oracle's own one-ulp sensitivity bound on DUDG), getq (hdgx_getq) against the oracle's
+restatement of kernel/getq.m, and one DIRK step (hdg_b200.dirk) against the oracle's
+restatement of kernel/hdg_solve_dirk.m: each stage is a Newton solve to 1e-10, so the step's
+states agree to 1e-8 relative."""
 import copy
 
 import numpy as np
@@ -67,3 +68,26 @@ def test_dirk_step_matches_oracle(oracle, q, p):
     assert relerr(Hn, Hn_ref) < 1e-8
     # the step moved the state (a time step, not a steady solve)
     assert relerr(Un, np.asarray(P.UDG)) > 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw", [("c1", dict(n=4, porder=2)), ("c2", dict(n=4, porder=3)), ("c4", dict(n=2, porder=2))])
+def test_getq_matches_oracle(oracle, name, kw):
+    """hdgx_getq (kernel/getq.m) against the oracle's restatement, with a q source and fc_q != 1
+    and without a source.  Like the q part of DUDG, getq is a small difference of O(1) volume and
+    face terms, inv(M) (C u - E uh): the bound is max(1e-12, 10 x the oracle's own change when
+    dgnodes, UDG and UH move by one ulp), as for DUDG in the elemental tests."""
+    from hdg_b200.elemental import getq
+    P = configs.by_name(name, **kw)
+    rng = np.random.default_rng(12)
+    SH = np.zeros_like(P.UDG)
+    SH[:, P.app.ncu:, :] = rng.standard_normal(SH[:, P.app.ncu:, :].shape)
+    jit = lambda x: x * (1.0 + 2.2e-16 * rng.standard_normal(x.shape))
+    for sh, fc_q in ((SH, 0.7), (None, 1.0)):
+        ref = oracle.getq(P.master, P.app, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), sh, fc_q)
+        ref1 = oracle.getq(P.master, P.app, jit(P.mesh.dgnodes), P.mesh.bf, jit(P.UDG), jit(P.uh_elem()), sh, fc_q)
+        bound = max(1e-12, 10.0 * relerr(ref1, ref))
+        Q, st = getq(P.master, P.app, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), sh, fc_q=fc_q)
+        assert int(st.numpy().max()) == 0
+        err = relerr(Q.numpy(), ref)
+        assert err < bound, f"{name} fc_q={fc_q} relerr {err:.3e} > {bound:.3e}"

@@ -13,7 +13,10 @@
                         (compiled the same way) on the blocks stored in ref_schur.npz; the u
                         form both on the D block alone and on the full BD / GK (nc > ncu).
 
-Usage: python tests/golden/make_golden.py [reference-root] [--only adjoint]
+* binfile_format.json -- the header positions (ndims(k) = ...) and the fwrite sequence of the
+                        single-process branch of util/writeBinaryFile.m, read from its source.
+
+Usage: python tests/golden/make_golden.py [reference-root] [--only adjoint|binfile]
 """
 import sys
 from pathlib import Path
@@ -56,6 +59,18 @@ def adjoint_fixture():
             for k, v in zip(("DUDG", "DUDG_DUH", "AE", "FE"), outs):
                 adj[f"{tag}_{form}_{k}"] = v
     np.savez_compressed(OUT / "ref_schur_adjoint.npz", **adj)
+
+
+def binfile_fixture(ref):
+    import json
+    import re
+    src = (Path(ref) / "util/writeBinaryFile.m").read_text()
+    start = src.index("if nproc == 1")
+    block = src[start:src.index("fclose(fileID);", start)]
+    code = "\n".join(line.split("%")[0] for line in block.splitlines())
+    header = {int(k): v.strip() for k, v in re.findall(r"ndims\((\d+)\)\s*=\s*([^;]+);", code)}
+    fwrites = [v.strip() for v in re.findall(r"fwrite\(fileID,\s*([^,]+),'double',endian\);", code)]
+    (OUT / "binfile_format.json").write_text(json.dumps({"header": header, "fwrites": fwrites}, indent=1) + "\n")
 
 
 def main(ref):
@@ -110,14 +125,18 @@ def main(ref):
             sch[f"{tag}_u_{k}"] = v
     np.savez_compressed(OUT / "ref_schur.npz", **sch)
     adjoint_fixture()
+    binfile_fixture(ref)
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
 
 
 if __name__ == "__main__":
     args = [x for x in sys.argv[1:] if not x.startswith("--only")]
-    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1:][:1] == ["adjoint"]:
-        args = [x for x in args if x != "adjoint"]
+    only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
+    args = [x for x in args if x != only]
+    if only == "adjoint":
         adjoint_fixture()
+    elif only == "binfile":
+        binfile_fixture(args[0] if args else "/root/reference")
     else:
         main(args[0] if args else "/root/reference")

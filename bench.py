@@ -24,6 +24,7 @@ import time
 from pathlib import Path
 
 import numpy as np
+import psutil
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
@@ -332,47 +333,59 @@ def main():
                 "algorithmic_bytes_per_element": cnt["bytes"],
                 "hbm": {"achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": achieved_gbs / peaks["hbm_gbs"], "peak_source": peak_kind}}
-        # end to end through the public host-array entry point (hdgx_elemental_host: pinned host
-        # inputs and outputs, the library overlaps uploads, kernel and downloads in chunks),
-        # every copy inside the timed region
-        from hdg_b200.elemental import alloc_host_outputs, hdg_elemental_host
-        h_in = {k: DArray(v.t.cpu().pin_memory(), v.shape) for k, v in d_in.items()}
-        h_out = alloc_host_outputs(m, a, ne)
+        out_bytes = sum(x.t.numel() * x.t.element_size() for x in (out.AE, out.FE, out.DUDG, out.DUDG_DUH))
+        avail = psutil.virtual_memory().available
+        e2e = None
+        if out_bytes > 0.5 * avail:
+            e2e = {"value": None, "unit": UNIT,
+                   "skipped": f"{out_bytes / 1e9:.1f} GB of pinned host outputs > half of the host's free memory"}
+        else:
+            # end to end through the public host-array entry point (hdgx_elemental_host: pinned host
+            # inputs and outputs, the library overlaps uploads, kernel and downloads in chunks),
+            # every copy inside the timed region
+            from hdg_b200.elemental import alloc_host_outputs, hdg_elemental_host
+            h_in = {k: DArray(v.t.cpu().pin_memory(), v.shape) for k, v in d_in.items()}
+            h_out = alloc_host_outputs(m, a, ne)
 
-        def e2e_step():
-            hdg_elemental_host(m, a, h_in["dg"], h_in["bf"], h_in["udg"], h_in["uh"], h_in["sh"], out=h_out,
-                               stream=stream, dmaster=dm, mixed=use_mixed)
-        e2e_step()                                   # warm-up: grows the library's device pool
-        ref_out = mixed_out if use_mixed else out
-        for k in ("FE", "DUDG", "status"):
-            if not torch.equal(getattr(h_out, k).t, getattr(ref_out, k).t.cpu()):
-                raise RuntimeError(f"host-array entry point differs from the device call in {k}")
-        e2e_steps = max(2, min(args.steps, 5))
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(e2e_steps):
-            e2e_step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms = e0.elapsed_time(e1) / e2e_steps
-        # the same copies issued one after another around the device call, for comparison
-        h_ser = [torch.empty_like(x.t, device="cpu").pin_memory() for x in (out.AE, out.FE, out.DUDG, out.DUDG_DUH)]
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(e2e_steps):
-            for k, v in d_in.items():
-                v.t.copy_(h_in[k].t, non_blocking=True)
-            step()
-            for h, x in zip(h_ser, (out.AE, out.FE, out.DUDG, out.DUDG_DUH)):
-                h.copy_(x.t, non_blocking=True)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        serial_ms = e0.elapsed_time(e1) / e2e_steps
-        del h_ser
-        h2d = sum(v.t.numel() * v.t.element_size() for v in d_in.values())
-        d2h = sum(x.t.numel() * x.t.element_size() for x in (h_out.AE, h_out.FE, h_out.DUDG, h_out.DUDG_DUH,
-                                                             h_out.status))
+            def e2e_step():
+                hdg_elemental_host(m, a, h_in["dg"], h_in["bf"], h_in["udg"], h_in["uh"], h_in["sh"], out=h_out,
+                                   stream=stream, dmaster=dm, mixed=use_mixed)
+            e2e_step()                                   # warm-up: grows the library's device pool
+            ref_out = mixed_out if use_mixed else out
+            for k in ("FE", "DUDG", "status"):
+                if not torch.equal(getattr(h_out, k).t, getattr(ref_out, k).t.cpu()):
+                    raise RuntimeError(f"host-array entry point differs from the device call in {k}")
+            e2e_steps = max(2, min(args.steps, 5))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(e2e_steps):
+                e2e_step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms = e0.elapsed_time(e1) / e2e_steps
+            # the same copies issued one after another around the device call, for comparison
+            # (into the same pinned buffers: C4's outputs alone are 61 GB of host memory)
+            h_ser = [h_out.AE.t, h_out.FE.t, h_out.DUDG.t, h_out.DUDG_DUH.t]
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(e2e_steps):
+                for k, v in d_in.items():
+                    v.t.copy_(h_in[k].t, non_blocking=True)
+                step()
+                for h, x in zip(h_ser, (out.AE, out.FE, out.DUDG, out.DUDG_DUH)):
+                    h.copy_(x.t, non_blocking=True)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            serial_ms = e0.elapsed_time(e1) / e2e_steps
+            h2d = sum(v.t.numel() * v.t.element_size() for v in d_in.values())
+            d2h = sum(x.t.numel() * x.t.element_size() for x in (h_out.AE, h_out.FE, h_out.DUDG, h_out.DUDG_DUH,
+                                                                 h_out.status))
+            e2e = {"value": ne / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                   "call": "hdgx_elemental_host (pinned host arrays, chunked and overlapped)",
+                   "d2h_gbs": d2h / (e2e_ms * 1e-3) / 1e9,
+                   "serial_copies_ms_per_step": serial_ms}
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
             nth = os.cpu_count() or 1
@@ -389,11 +402,7 @@ def main():
                        "elements_per_gpu": ne, "parallelism": f"replicas x{ws} (elements independent)",
                        "l2": f"each step writes {d2h / 1e9:.2f} GB of outputs (> 126 MB L2), evicting the inputs"},
             "roofline": roof, "cpu_baseline": cpu,
-            "e2e": {"value": ne / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                    "call": "hdgx_elemental_host (pinned host arrays, chunked and overlapped)",
-                    "d2h_gbs": d2h / (e2e_ms * 1e-3) / 1e9,
-                    "serial_copies_ms_per_step": serial_ms},
+            "e2e": e2e,
             "clocks": clocks, "gpu_launches": args.steps,
             "kernel_ms": {"mean": statistics.mean(kern_ms), "min": min(kern_ms), "max": max(kern_ms)},
         }
@@ -407,6 +416,10 @@ def main():
                       "scheme": "FP32 local elimination of the Jacobian columns, FP64-refined residual solve, FP64 residuals"},
             "mixed_over_fp64": fp64_ms / mixed_ms,
         }
+        # the elemental step's device buffers (C4: two 61 GB output sets) are not needed below
+        out = mixed_out = d_in = None
+        step = step_fp64 = step_mixed = other = None
+        torch.cuda.empty_cache()
         if not args.no_newton and ws == 1:
             line["newton"] = newton_step(P, torch, args)
         if not args.no_buckets and ws == 1:

@@ -142,3 +142,26 @@ def test_host_array_entry_point_rejects_bad_arguments():
                                      None) == -1
     assert lib().hdgx_elemental_host(ct.byref(dm.c), ct.byref(a), 0, p, p, p, p, p, p, p, p, p, None, 0, 0,
                                      None) == 0
+
+
+@pytest.mark.gpu
+def test_host_array_entry_point_accepts_pageable_memory():
+    """hdgx_elemental_host on plain (pageable) numpy buffers through the C ABI: the driver stages
+    the copies, the results are still bitwise those of the device call."""
+    import ctypes as ct
+    from hdg_b200._lib import lib
+    from hdg_b200.elemental import DeviceMaster, app_struct, hdg_elemental
+    P = configs.c2(n=4, porder=3)
+    m, a = P.master, P.app
+    dev = hdg_elemental(m, a, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), P.SH)
+    F = lambda x, t=np.float64: np.ascontiguousarray(np.asarray(x, dtype=t).ravel(order="F"))
+    ins = [F(P.mesh.dgnodes), F(P.mesh.bf, np.int32), F(P.UDG), F(P.uh_elem()), F(P.SH)]
+    outs = [np.zeros(getattr(dev, k).t.numel()) for k in ("AE", "FE", "DUDG", "DUDG_DUH")]
+    st = np.full(P.mesh.ne, -1, dtype=np.int32)
+    dm, ac = DeviceMaster(m), app_struct(a)
+    rc = lib().hdgx_elemental_host(ct.byref(dm.c), ct.byref(ac), P.mesh.ne, *[x.ctypes.data for x in ins],
+                                   *[x.ctypes.data for x in outs], st.ctypes.data, 0, 7, None)
+    assert rc == 0
+    assert np.all(st == 0)
+    for k, o in zip(("AE", "FE", "DUDG", "DUDG_DUH"), outs):
+        assert np.array_equal(o, getattr(dev, k).t.cpu().numpy()), k

@@ -83,7 +83,7 @@ int check_elemental(const hdgx_master *master, const hdgx_app *app, int ne, cons
     const int nd = master->nd;
     if (app->nd != nd || app->ncu != nd + 2 || app->nc != (nd + 2) * (nd + 1) || master->nfe != nd + 1)
         return -2;
-    if (app->localsolve != 1 || app->getdqdg != 1) return -2;
+    if (app->localsolve != 1 || (app->getdqdg != 0 && app->getdqdg != 1)) return -2;
     if (app->nbnd < 0 || app->nbnd > HDGX_MAX_BND) return -4;
     return 0;
 }
@@ -205,11 +205,13 @@ int hdgx_elemental_host(const hdgx_master *master, const hdgx_app *app, int ne, 
     const size_t npv = master->npv, nd = master->nd, nfe = master->nfe, nc = app->nc, ncu = app->ncu;
     const size_t ndf = (size_t)master->npf * nfe;
     // doubles (ints for bf, status) per element of every array, in argument order
-    const size_t n_x = npv * nd, n_u = npv * nc, n_h = ncu * ndf, n_ae = n_h * n_h, n_dd = n_u * n_h;
+    const size_t nco = app->getdqdg ? nc : ncu;       // components of DUDG / DUDG_DUH
+    const size_t n_x = npv * nd, n_u = npv * nc, n_h = ncu * ndf, n_ae = n_h * n_h, n_o = npv * nco,
+                 n_dd = n_o * n_h;
     if (chunk == 0) chunk = ne < 16 * 1024 ? (ne < 1024 ? ne : 1024) : (ne + 15) / 16;
     if (chunk > ne) chunk = ne;
     // one staging set: every array of `chunk` elements, each on a 256-byte boundary
-    const size_t dbl[8] = {n_x, n_u, n_h, n_u, n_ae, n_h, n_u, n_dd}, ints[2] = {nfe, 1};
+    const size_t dbl[8] = {n_x, n_u, n_h, n_u, n_ae, n_h, n_o, n_dd}, ints[2] = {nfe, 1};
     auto rnd = [](size_t bytes) { return (bytes + 255) & ~(size_t)255; };
     size_t set_bytes = 0;
     for (size_t d : dbl) set_bytes += rnd(sizeof(double) * d * chunk);
@@ -274,7 +276,7 @@ int hdgx_elemental_host(const hdgx_master *master, const hdgx_app *app, int ne, 
             ok(cudaStreamWaitEvent(s_out, ev_k[b], 0));
             d2h(AE, S.ae, sizeof(double) * n_ae);
             d2h(FE, S.fe, sizeof(double) * n_h);
-            d2h(DUDG, S.dd, sizeof(double) * n_u);
+            d2h(DUDG, S.dd, sizeof(double) * n_o);
             d2h(DUDG_DUH, S.ddh, sizeof(double) * n_dd);
             if (status) d2h(status, S.status, sizeof(int));
             ok(cudaEventRecord(ev_out[b], s_out));

@@ -38,6 +38,7 @@ struct ElemParams {
     double *AE, *FE, *DUDG, *DUDG_DUH;
     int *status;
     double *QDG;               // non-NULL: getq mode (kernel/getq.m), the element stops after inv(M)
+    int nco;                   // components stored in DUDG / DUDG_DUH: nc, or ncu when app.getdqdg = 0
 };
 
 template <int ND_, int NPV_, int NPF_, int NGV_, int NGF_>
@@ -751,7 +752,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
 
         // ================================ DUDG = [du, MiRq + MiC du] (schur_primal.m:112-116)
         {
-            double *g_dudg = P.DUDG + (size_t)e * NQ;
+            double *g_dudg = P.DUDG + (size_t)e * NPV * P.nco;
             for (int i = tid; i < NQ; i += NT) {
                 const int r = i % NPV, c = i / NPV;
                 double v;
@@ -764,7 +765,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * s_R[s + NPV * a];
                 }
                 s_dudg[i] = v;
-                g_dudg[i] = v;
+                if (c < P.nco) g_dudg[i] = v;       // getdqdg = 0: the u rows only
             }
         }
         __syncthreads();
@@ -804,7 +805,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             constexpr int T = L::TILE;
             constexpr int TMQ = NPV <= 6 ? NPV : (NPV + 1) / 2;
             double *yX = sm + L::y_X, *yXg = sm + L::y_Xg, *yY = sm + L::y_Y;
-            double *g_dd = P.DUDG_DUH + (size_t)e * NQ * NH;
+            double *g_dd = P.DUDG_DUH + (size_t)e * NPV * P.nco * NH;   // [npv, nco, ncu, ndf]
             double *g_ae = P.AE + (size_t)e * NH * NH;
             for (int k0 = 0; k0 < NH; k0 += T) {
                 const int nt = (NH - k0) < T ? (NH - k0) : T;
@@ -812,7 +813,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     const int ru = i % NU, t = i / NU;
                     const double v = s_R[NU * (1 + k0 + t) + ru];
                     yX[ru + NQ * t] = v;
-                    g_dd[(size_t)NQ * (k0 + t) + ru] = v;
+                    g_dd[(size_t)NPV * P.nco * (k0 + t) + ru] = v;
                 }
                 // q rows r + NPV (NCU + a + NCU d) of column k = k0 + t, batch d, n = (a, t)
                 tile_gemm<ND, NPV, NCU * T, NPV, TMQ, 2, NT>(
@@ -828,7 +829,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                         if (a == k % NCU) v -= s_MiE[r + NPV * (k / NCU + NDF * d)];
                         const int row = r + NPV * (NCU + a + NCU * d);
                         yX[row + NQ * t] = v;
-                        g_dd[(size_t)NQ * k + row] = v;
+                        if (P.nco == NC) g_dd[(size_t)NQ * k + row] = v;
                     });
                 __syncthreads();
                 // Xg(gg, c, t) = sum_m shapft(g, m) X(perm(m, j), c, t), batch j, n = (c, t)
@@ -920,6 +921,7 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
     p.ne = ne; p.dgnodes = dgnodes; p.UDG = UDG; p.UH = UH; p.SH = SH; p.bf = bf;
     p.AE = AE; p.FE = FE; p.DUDG = DUDG; p.DUDG_DUH = DUDG_DUH; p.status = status;
     p.QDG = QDG;
+    p.nco = app->getdqdg ? app->nc : app->ncu;
     const bool visc = p.pc.rinv != 0.0;
     const int nd = m->nd, po = m->porder;
     if (nd == 2) {

@@ -240,6 +240,7 @@ extern "C" int hdgx_solve(const hdgx_master *m, const hdgx_app *app, const hdgx_
     if (!mesh->dgnodes || !mesh->bf || !mesh->elcon || !mesh->t2f || !mesh->rowpts || !mesh->colind) return -1;
     const int ne = mesh->ne, nf = mesh->nf;
     if (ne < 1 || nf < 1 || opts->restart < 1 || opts->maxiter < 0 || opts->gmres_maxit < 1) return -1;
+    if (app->getdqdg != 1) return -2;    // the native loop keeps q in the local solve (getdqdg = 1)
     if (opts->ordering != 0 && opts->ordering != 1) return -1;
     cudaStream_t st = (cudaStream_t)stream;
     const int npv = m->npv, npf = m->npf, nfe = m->nfe, ncu = app->ncu, nc = app->nc;
@@ -268,7 +269,12 @@ extern "C" int hdgx_solve(const hdgx_master *m, const hdgx_app *app, const hdgx_
     double *UDG0 = pool.get<double>(nU), *UH0 = pool.get<double>(nH);
     double *part = pool.get<double>(1024 + 8);
     int *status = pool.get<int>(ne);
+    // hdg_solve.m:62-63: without the wave formulation the q part of SH is zero
+    double *SHz = pool.get<double>(nU);
     if (pool.failed) return -13;
+    cudaMemcpyAsync(SHz, SH, sizeof(double) * nU, cudaMemcpyDeviceToDevice, st);
+    cudaMemset2DAsync(SHz + (size_t)npv * ncu, sizeof(double) * npv * nc, 0, sizeof(double) * npv * (nc - ncu), ne, st);
+    SH = SHz;
 
     hdgx_bsr A = {};
     A.nf = nf;

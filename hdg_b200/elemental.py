@@ -119,11 +119,16 @@ class ElementalOutputs:
         return iter((self.AE, self.FE, self.DUDG, self.DUDG_DUH))
 
 
+def stored_components(app):
+    """Components of DUDG / DUDG_DUH: nc, or ncu when app.getdqdg = 0 (hdg_elemental.m:20-26)."""
+    return app.nc if getattr(app, "getdqdg", 1) else app.ncu
+
+
 def alloc_elemental_outputs(master, app, ne):
-    npv, ncu, nc = master.npv, app.ncu, app.nc
+    npv, ncu, nco = master.npv, app.ncu, stored_components(app)
     ndf = master.npf * master.nfe
     return ElementalOutputs(DArray.empty((ncu, ndf, ncu, ndf, ne)), DArray.empty((ncu, ndf, ne)),
-                            DArray.empty((npv, nc, ne)), DArray.empty((npv, nc, ncu, ndf, ne)),
+                            DArray.empty((npv, nco, ne)), DArray.empty((npv, nco, ncu, ndf, ne)),
                             DArray.zeros((ne,), dtype=torch.int32))
 
 
@@ -193,7 +198,7 @@ def as_host_darray(x, dtype=torch.float64):
 
 def alloc_host_outputs(master, app, ne):
     """Page-locked host outputs of hdg_elemental_host."""
-    npv, ncu, nc = master.npv, app.ncu, app.nc
+    npv, ncu, nc = master.npv, app.ncu, stored_components(app)
     ndf = master.npf * master.nfe
 
     def pinned(shape, dtype=torch.float64):

@@ -20,8 +20,8 @@ import numpy as np
 import torch
 
 from ._lib import HdgxAssemblyMap, HdgxBsr, check, lib
-from .elemental import (DArray, DeviceMaster, alloc_elemental_outputs, app_struct, as_darray, _require_cuda,
-                        _stream_ptr)
+from .elemental import (DArray, DeviceMaster, alloc_elemental_outputs, app_struct, as_darray, getq, _require_cuda,
+                        _stream_ptr, stored_components)
 from .ordering import assembly_map, levels_of_order, multicolor, sweep_plan
 
 
@@ -188,7 +188,8 @@ class HDGSolver:
         self.work = self.ts.empty_vec()
         ndf = master.npf * master.nfe
         self.UHe = DArray.empty((app.ncu, ndf, ne))
-        self.DUDGT = DArray.empty((master.npv, app.nc, ne))
+        self.nco = stored_components(app)             # nc, or ncu when app.getdqdg = 0
+        self.DUDGT = DArray.empty((master.npv, self.nco, ne))
         self.app_c = app_struct(app)
         self.restart = restart
         self.denseblock = denseblock
@@ -230,8 +231,25 @@ class HDGSolver:
         m, a = self.master, self.app
         ndf = m.npf * m.nfe
         o = self.out
-        check(lib().hdgx_backsub(m.npv, a.nc, a.ncu, ndf, self.ne, self.ts.d["elcon"].ptr, o.DUDG.ptr,
+        check(lib().hdgx_backsub(m.npv, self.nco, a.ncu, ndf, self.ne, self.ts.d["elcon"].ptr, o.DUDG.ptr,
                                  o.DUDG_DUH.ptr, self.DUH.ptr, self.DUDGT.ptr, _stream_ptr(stream)), "hdgx_backsub")
+
+    def update(self, UDG, UH, UDG0, UH0, alfa, SH):
+        """UDG(:,1:nco,:) = UDG0 + alfa DUDGT, UH = UH0 + alfa DUH (hdg_solve.m:145-146); with
+        app.getdqdg = 0 the q part is then recovered with getq (hdg_solve.m:148-151)."""
+        if self.nco == self.app.nc:
+            torch.add(UDG0, self.DUDGT.t, alpha=alfa, out=UDG.t)
+        else:
+            ne, npv, nc, nco = self.ne, self.master.npv, self.app.nc, self.nco
+            u = UDG.t.view(ne, nc, npv)
+            u.copy_(UDG0.view(ne, nc, npv))
+            u[:, :nco, :].add_(self.DUDGT.t.view(ne, nco, npv), alpha=alfa)
+        torch.add(UH0, self.DUH.t.view(-1), alpha=alfa, out=UH.t)
+        if self.nco != self.app.nc:
+            self.gather(UH)
+            Q, _ = getq(self.master, self.app, self.dg, self.bf, UDG, self.UHe, SH, dmaster=self.dm)
+            ne, npv, nc, ncu = self.ne, self.master.npv, self.app.nc, self.app.ncu
+            UDG.t.view(ne, nc, npv)[:, ncu:, :].copy_(Q.t.view(ne, nc - ncu, npv))
 
     def solve(self, UDG, UH, SH, tol=1e-10, maxiter=16, gmres_tol=1e-10, gmres_maxit=1000, linear=False):
         """The Newton loop of hdg_solve.m; UDG [npv,nc,ne], UH [ncu,nsiz] device arrays (updated)."""
@@ -250,8 +268,9 @@ class HDGSolver:
             rep.gmres_relres.append(grr)
             self.backsub()
             if linear:
-                UDG.t.add_(self.DUDGT.t)
-                UH.t.add_(self.DUH.t.view(-1))
+                UDG0.copy_(UDG.t)
+                UH0.copy_(UH.t)
+                self.update(UDG, UH, UDG0, UH0, 1.0, SH)
                 rep.iterations = 1
                 return rep
             it += 1
@@ -260,8 +279,7 @@ class HDGSolver:
             duh0 = F
             alfa = 1.0
             while True:
-                torch.add(UDG0, self.DUDGT.t, alpha=alfa, out=UDG.t)
-                torch.add(UH0, self.DUH.t.view(-1), alpha=alfa, out=UH.t)
+                self.update(UDG, UH, UDG0, UH0, alfa, SH)
                 F = self.assemble(UDG, UH, SH)
                 if F > duh0:
                     alfa /= 2
@@ -290,7 +308,9 @@ def hdg_solve(master, mesh, app, UDG, UH, SH=None, tol=1e-10, maxiter=16, gmres_
     s = HDGSolver(master, mesh, app, ordering=ordering, restart=restart, mixed=mixed, denseblock=denseblock)
     dU = DArray.from_numpy(UDG)
     dH = DArray.from_numpy(UH)
-    dS = DArray.from_numpy(np.zeros_like(UDG) if SH is None else SH)
+    SH = np.zeros_like(UDG) if SH is None else np.array(SH, dtype=np.float64, copy=True)
+    SH[:, app.ncu:, :] = 0.0                     # hdg_solve.m:62-63 (no wave formulation here)
+    dS = DArray.from_numpy(SH)
     rep = s.solve(dU, dH, dS, tol=tol, maxiter=maxiter, gmres_tol=gmres_tol)
     return dU.numpy(), dH.numpy(), rep
 

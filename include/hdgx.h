@@ -62,7 +62,8 @@ typedef struct {
 typedef struct {
     int nd, ncu, nc;        /* nc = ncu*(nd+1) for the (u,q) form */
     int localsolve;         /* 1: (u,q) form (only form the fused kernel supports) */
-    int getdqdg;            /* 1: DUDG/DUDG_DUH carry all nc components (reference default) */
+    int getdqdg;            /* 1: DUDG/DUDG_DUH carry all nc components (reference default); 0: the u
+                               components only, q is recovered with hdgx_getq (hdg_solve.m:129-132) */
     double fc_q, fc_u;      /* fc_u: time-derivative coefficient of a DIRK stage (tdep = 1) */
     int tdep;               /* 1: time-dependent residual of kernel/volint.m:180-221 (dtcoef = 1, no
                                axisymmetry): source SH_u - fc_u u, Jacobian -fc_u on the u components */
@@ -82,8 +83,9 @@ int hdgx_status_count(const int *status, int n, hdgx_stream_t stream);
 /* Fused FP64 elemental kernel: volume + face integrals + local (u,q) Schur elimination.
  * Inputs : dgnodes[npv,nd,ne], bf[nfe,ne] (int32), UDG[npv,nc,ne], UH[ncu,npf*nfe,ne]
  *          (element-gathered trace), SH[npv,nc,ne].
- * Outputs: AE[ncu,ndf,ncu,ndf,ne], FE[ncu,ndf,ne], DUDG[npv,nc,ne], DUDG_DUH[npv,nc,ncu,ndf,ne]
- *          (ndf = npf*nfe), status[ne] (may be NULL).
+ * Outputs: AE[ncu,ndf,ncu,ndf,ne], FE[ncu,ndf,ne], DUDG[npv,nco,ne], DUDG_DUH[npv,nco,ncu,ndf,ne]
+ *          (ndf = npf*nfe; nco = nc, or ncu when app->getdqdg = 0: the u rows only, as
+ *          hdg_elemental.m:20-26 sizes them), status[ne] (may be NULL).
  * Supported (nd, porder): 2D 1..4, 3D 1..2; returns -3 otherwise. */
 int hdgx_elemental(const hdgx_master *master, const hdgx_app *app, int ne,
                    const double *dgnodes, const int *bf, const double *UDG, const double *UH,
@@ -319,8 +321,9 @@ typedef struct {
 /* Newton solve of kernel/hdg_solve.m:84-176 on the device: assembly (hdg_assemble.m), BILU(0)-
  * GMRES with x0 = 0 in place of K\F, back-substitution (hdg_solve.m:119-121) and the halving
  * line search (hdg_solve.m:144-163), until |F| / |F0| <= tol or maxiter steps.  UDG [npv,nc,ne]
- * and UH [ncu, nf*npf] (device) are updated in place; SH [npv,nc,ne] (device) is the source.
- * Workspace comes from a private stream-ordered memory pool of the library (one per device) and
+ * and UH [ncu, nf*npf] (device) are updated in place; SH [npv,nc,ne] (device) is the source,
+ * whose q part is taken as zero (hdg_solve.m:62-63, no wave formulation).  app->getdqdg must be
+ * 1 (returns -2 otherwise; the Python composition also runs getdqdg = 0).  Workspace comes from a private stream-ordered memory pool of the library (one per device) and
  * is released into it before returning; the pool keeps up to 8 GiB of freed memory for later
  * calls.  The call synchronises the stream (it reads residual norms on the host). */
 int hdgx_solve(const hdgx_master *master, const hdgx_app *app, const hdgx_mesh *mesh, double *UDG, double *UH,

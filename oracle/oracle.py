@@ -97,6 +97,9 @@ def hdg_elemental(master, app, dgnodes, bf, UDG, UH, SH, intermediates=False, nt
                                _p(uh), _p(sh), _p(AE), _p(FE), _p(DUDG), _p(DUDG_DUH),
                                g("M"), g("C"), g("E"), g("BD"), g("F"), g("GK"), g("H"), g("Rq"),
                                g("Ru"), g("Rh"), st.ctypes.data_as(_ip), int(nthreads))
+    if not getattr(app, "getdqdg", 1):       # hdg_elemental.m:20-26: nco = ncu, the u rows only
+        ncu = app.ncu
+        DUDG, DUDG_DUH = np.asfortranarray(DUDG[:, :ncu]), np.asfortranarray(DUDG_DUH[:, :ncu])
     out = dict(AE=AE, FE=FE, DUDG=DUDG, DUDG_DUH=DUDG_DUH, status=st, nbad=nbad)
     out.update(blk)
     return out
@@ -273,10 +276,12 @@ def hdg_solve(P, o2u=None, u2o=None, tol=1e-10, maxiter=16, gmres_tol=1e-10, res
     npf, ncu = m.npf, a.ncu
     UDG = np.array(P.UDG, order="F", copy=True)
     UH = np.array(P.UH, order="F", copy=True)
+    SH = np.array(P.SH, order="F", copy=True)
+    SH[:, ncu:, :] = 0.0                         # hdg_solve.m:62-63 (app.wave == 0)
 
     def assemble(UDG, UH):
         from hdg_b200.app import gather_uh
-        r = hdg_elemental(m, a, mesh.dgnodes, mesh.bf, UDG, gather_uh(UH, mesh.elcon), P.SH, nthreads=nthreads)
+        r = hdg_elemental(m, a, mesh.dgnodes, mesh.bf, UDG, gather_uh(UH, mesh.elcon), SH, nthreads=nthreads)
         Hg, Rg = globalassembly(mesh, r["AE"], r["FE"], npf, ncu)
         return r, Hg, Rg
 
@@ -298,9 +303,14 @@ def hdg_solve(P, o2u=None, u2o=None, tol=1e-10, maxiter=16, gmres_tol=1e-10, res
         it += 1
         UDG0, UH0, duh0 = UDG.copy(), UH.copy(), F
         alfa = 1.0
+        nco = DUDGT.shape[1]
         while True:
-            UDG = UDG0 + alfa * DUDGT
+            UDG = UDG0.copy()
+            UDG[:, :nco, :] += alfa * DUDGT                      # hdg_solve.m:145-146
             UH = UH0 + alfa * DUH
+            if nco < a.nc:                                        # getdqdg = 0: hdg_solve.m:148-151
+                from hdg_b200.app import gather_uh
+                UDG[:, ncu:, :] = getq(m, a, mesh.dgnodes, mesh.bf, UDG, gather_uh(UH, mesh.elcon), SH, a.fc_q)
             r, Hg, Rg = assemble(UDG, UH)
             F = float(np.linalg.norm(Rg))
             if F > duh0:

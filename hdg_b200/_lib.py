@@ -103,6 +103,8 @@ def _declare(L):
     L.hdgx_schur_uq.argtypes = [i] * 5 + [v] * 15 + [v]
     L.hdgx_getq.restype = i
     L.hdgx_getq.argtypes = [p(HdgxMaster), p(HdgxApp), i] + [v] * 7 + [v]
+    L.hdgx_residual.restype = i
+    L.hdgx_residual.argtypes = [p(HdgxMaster), p(HdgxApp), i] + [v] * 7 + [v]
     L.hdgx_schur_uq_adjoint.restype = i
     L.hdgx_schur_uq_adjoint.argtypes = [i] * 5 + [v] * 15 + [v]
     L.hdgx_schur_u_adjoint.restype = i

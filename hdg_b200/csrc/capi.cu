@@ -8,7 +8,7 @@ namespace hdgx {
 int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const double *dgnodes,
                      const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
                      double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed,
-                     int grid, double *QDG = nullptr);
+                     int grid, double *QDG = nullptr, double *RU = nullptr);
 cudaMemPool_t device_pool();
 int schur_adjoint_launch(int qform, int nd, int npv, int ncu, int nc, int ndf, int ne, const double *M,
                          const double *C, const double *E, const double *BD, const double *F, const double *GK,
@@ -149,6 +149,23 @@ int hdgx_getq(const hdgx_master *master, const hdgx_app *app, int ne, const doub
     if (!(app->fc_q != 0.0)) return -1;
     return hdgx::elemental_launch(master, app, ne, dgnodes, bf, UDG, UH, SH, nullptr, nullptr, nullptr, nullptr,
                                   status, (cudaStream_t)stream, false, 0, QDG);
+}
+
+int hdgx_residual(const hdgx_master *master, const hdgx_app *app, int ne, const double *dgnodes, const int *bf,
+                  const double *UDG, const double *UH, const double *SH, double *Ru, int *status,
+                  hdgx_stream_t stream) {
+    if (!master || !app || ne < 0) return -1;
+    if (ne == 0) return 0;
+    if (!dgnodes || !bf || !UDG || !UH || !Ru) return -1;
+    if (!master->shapvt || !master->shapvg || !master->shapmv || !master->shapft || !master->shapfg ||
+        !master->shapmf || !master->perm)
+        return -1;
+    const int nd = master->nd;
+    if (app->nd != nd || app->ncu != nd + 2 || app->nc != (nd + 2) * (nd + 1) || master->nfe != nd + 1) return -2;
+    if (app->nbnd < 0 || app->nbnd > HDGX_MAX_BND) return -4;
+    if (!(app->fc_q != 0.0)) return -1;
+    return hdgx::elemental_launch(master, app, ne, dgnodes, bf, UDG, UH, SH, nullptr, nullptr, nullptr, nullptr,
+                                  status, (cudaStream_t)stream, false, 0, nullptr, Ru);
 }
 
 int hdgx_elemental_buckets(int nb, const hdgx_elem_bucket *b, int mixed, hdgx_stream_t stream) {

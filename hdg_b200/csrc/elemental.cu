@@ -39,6 +39,7 @@ struct ElemParams {
     int *status;
     double *QDG;               // non-NULL: getq mode (kernel/getq.m), the element stops after inv(M)
     int nco;                   // components stored in DUDG / DUDG_DUH: nc, or ncu when app.getdqdg = 0
+    double *RU;                // non-NULL: residual mode (kernel/cuda_residual.m), Ru at q = getq(u, uh)
 };
 
 template <int ND_, int NPV_, int NPF_, int NGV_, int NGF_>
@@ -364,7 +365,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
 #pragma unroll
             for (int s = 0; s < NPV; s++)
                 t += s_M[r + NPV * s] * ((P.SH ? g_shq[s + NPV * (a + NCU * d)] / P.fc_q : 0.0) -
-                                         (P.QDG ? 0.0 : s_udg[s + NPV * cq]));   // getq: q does not enter
+                                         ((P.QDG || P.RU) ? 0.0 : s_udg[s + NPV * cq]));   // getq: q does not enter
 #pragma unroll
             for (int s = 0; s < NPV; s++) t += s_MiC[r + NPV * (s + NPV * d)] * s_udg[s + NPV * a];
             for (int f = 0; f < NDF; f++) t -= s_MiE[r + NPV * (f + NDF * d)] * s_uh[a + NCU * f];
@@ -385,6 +386,26 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             if (tid == 0 && P.status) P.status[e] = *s_bad;
             __syncthreads();
             continue;
+        }
+        if (P.RU) {
+            // cuda_residual.m:3-4: q from getq, then the u residual is evaluated at that q
+            for (int i = tid; i < NPV * NCU * ND; i += NT) s_udg[NPV * NCU + i] = s_MiRq[i];
+            __syncthreads();
+            for (int i = tid; i < NGV * NCU * ND; i += NT) {
+                const int g = i % NGV, c = NCU + i / NGV;
+                double t = 0.0;
+#pragma unroll
+                for (int n = 0; n < NPV; n++) t += t_vt[g + NGV * n] * s_udg[n + NPV * c];
+                x_ug[g + NGV * c] = t;
+            }
+            for (int i = tid; i < NGT * NCU * ND; i += NT) {
+                const int gg = i % NGT, c = NCU + i / NGT, g = gg % NGF, j = gg / NGF;
+                double t = 0.0;
+#pragma unroll
+                for (int n = 0; n < NPF; n++) t += t_ft[g + NGF * n] * s_udg[perm[n + NPF * j] + NPV * c];
+                x_fu[gg + NGT * c] = t;
+            }
+            __syncthreads();
         }
 
         // ================================ flux / fhat / fbou at the Gauss points
@@ -574,8 +595,9 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                 for (int id = 0; id < ND; id++) {
                     double w = x_wrk[g + NGV * (id + ND * a)];
                     if constexpr (VISC) {
-                        for (int bd = 0; bd < NCU * ND; bd++)
-                            w -= x_wrl[g + NGV * (id + ND * (a + NCU * (NCU + bd)))] * x_Zr[g + NGV * bd];
+                        if (!P.RU)                     // residual mode: Rq = 0 at q = getq
+                            for (int bd = 0; bd < NCU * ND; bd++)
+                                w -= x_wrl[g + NGV * (id + ND * (a + NCU * (NCU + bd)))] * x_Zr[g + NGV * bd];
                     }
                     v += t_vg[r + NPV * (g + NGV * (id + 1))] * w;
                 }
@@ -587,8 +609,9 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     const int gg = g + NGF * j;
                     double w = -x_FH[gg + NGT * a];
                     if constexpr (VISC) {
-                        for (int bd = 0; bd < NCU * ND; bd++)
-                            w -= x_FHu[gg + NGT * (a + NCU * (NCU + bd))] * x_ZFr[gg + NGT * bd];
+                        if (!P.RU)
+                            for (int bd = 0; bd < NCU * ND; bd++)
+                                w -= x_FHu[gg + NGT * (a + NCU * (NCU + bd))] * x_ZFr[gg + NGT * bd];
                     }
                     v += t_fg[m + NPF * g] * w;
                 }
@@ -641,6 +664,14 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             });
         };
         build_rhs();
+        if (P.RU) {
+            // cuda_residual.m: the element u residual Ru (volume and face terms, time source)
+            __syncthreads();
+            for (int i = tid; i < NU; i += NT) P.RU[(size_t)e * NU + i] = s_R[i];
+            if (tid == 0 && P.status) P.status[e] = *s_bad;
+            __syncthreads();
+            continue;
+        }
         // Rh = -(fbou or fhat) integrated on each face (faceint.m:335-339)
         for (int i = tid; i < NH; i += NT) {
             const int a = i % NCU, mf = i / NCU, m = mf % NPF, j = mf / NPF;
@@ -903,7 +934,7 @@ static int launch_v(const ElemParams &p, bool visc, bool mixed, cudaStream_t st,
 int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const double *dgnodes,
                      const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
                      double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed,
-                     int grid, double *QDG) {
+                     int grid, double *QDG, double *RU) {
     ElemParams p;
     p.shapvt = m->shapvt; p.shapvg = m->shapvg; p.shapmv = m->shapmv;
     p.shapft = m->shapft; p.shapfg = m->shapfg; p.shapmf = m->shapmf; p.perm = m->perm;
@@ -921,6 +952,7 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
     p.ne = ne; p.dgnodes = dgnodes; p.UDG = UDG; p.UH = UH; p.SH = SH; p.bf = bf;
     p.AE = AE; p.FE = FE; p.DUDG = DUDG; p.DUDG_DUH = DUDG_DUH; p.status = status;
     p.QDG = QDG;
+    p.RU = RU;
     p.nco = app->getdqdg ? app->nc : app->ncu;
     const bool visc = p.pc.rinv != 0.0;
     const int nd = m->nd, po = m->porder;

@@ -183,6 +183,25 @@ def getq(master, app, dgnodes, bf, UDG, UH, SH=None, fc_q=None, stream=None, dma
     return Q, st
 
 
+def residual(master, app, dgnodes, bf, UDG, UH, SH=None, stream=None, dmaster=None):
+    """kernel/cuda_residual.m: the element u residual Ru[npv, ncu, ne] at q = getq(u, uh), with
+    no Jacobian and no local solve (explicit / residual-only evaluation).  Returns (Ru, status)."""
+    _require_cuda()
+    L = lib()
+    dm = dmaster if dmaster is not None else DeviceMaster(master)
+    dg, udg, uh = (as_darray(x) for x in (dgnodes, UDG, UH))
+    sh = as_darray(SH) if SH is not None else None
+    bfd = as_darray(bf, dtype=torch.int32)
+    ne = udg.shape[-1]
+    Ru = DArray.empty((master.npv, app.ncu, ne))
+    st = DArray.zeros((ne,), dtype=torch.int32)
+    a = app_struct(app)
+    rc = L.hdgx_residual(ct.byref(dm.c), ct.byref(a), ne, dg.ptr, bfd.ptr, udg.ptr, uh.ptr, sh.ptr if sh else None,
+                         Ru.ptr, st.ptr, _stream_ptr(stream))
+    check(rc, "hdgx_residual")
+    return Ru, st
+
+
 def as_host_darray(x, dtype=torch.float64):
     """A column-major page-locked host DArray of ``x`` (a numpy array, or a host DArray kept as is)."""
     if isinstance(x, DArray):

@@ -17,6 +17,7 @@
  *   hdgx_schur_uq    kernel/schur_uq.c:193      [DUDG,DUDG_DUH,AE,FE] = schur_uq(M,C,E,BD,F,GK,H,Rq,Ru,Rh)
  *   hdgx_schur_u     kernel/schur_u.c:82        [DUDG,DUDG_DUH,AE,FE] = schur_u(BD,F,GK,H,Ru,Rh)
  *   hdgx_getq        kernel/getq.m:1            QDG = getq(master,mesh,UDG,UH,SH,fc_q)
+ *   hdgx_residual    kernel/cuda_residual.m:1   Ru = cuda_residual(...): Ru at q = getq(u, uh)
  *   hdgx_schur_uq_adjoint  kernel/schur_uq_adjoint.c:300  [DUDG,DUDG_DUH,AE,FE] = schur_uq_adjoint(M,C,E,BD,F,GK,H,Rq,Ru,Rh)
  *   hdgx_schur_u_adjoint   kernel/schur_u_adjoint.c:145   [DUDG,DUDG_DUH,AE,FE] = schur_u_adjoint(BD,F,GK,H,Ru,Rh)
  *   hdgx_globalassembly   kernel/globalassembly.m:1  [Hg,Rg] = globalassembly(mesh,AE,FE)
@@ -168,6 +169,15 @@ int hdgx_schur_u(int npv, int ncu, int nc, int ndf, int ne,
 int hdgx_getq(const hdgx_master *master, const hdgx_app *app, int ne, const double *dgnodes,
               const int *bf, const double *UDG, const double *UH, const double *SH, double *QDG,
               int *status, hdgx_stream_t stream);
+
+/* cuda_residual.m: the residual-only evaluation used by explicit time stepping.  q is first
+ * recovered from u and the trace (as hdgx_getq), then the element u residual Ru[npv,ncu,ne] is
+ * evaluated at that q: volume flux and (app->tdep = 1) time source terms plus the face fhat /
+ * fbou terms, the Ru of volint.m / faceint.m, with no Jacobian and no local solve.  Arguments as
+ * hdgx_getq; status as hdgx_elemental. */
+int hdgx_residual(const hdgx_master *master, const hdgx_app *app, int ne, const double *dgnodes,
+                  const int *bf, const double *UDG, const double *UH, const double *SH, double *Ru,
+                  int *status, hdgx_stream_t stream);
 
 /* Adjoint (transposed) local Schur complements, the reference's schur_uq_adjoint.c and
  * schur_u_adjoint.c on the same layouts and arguments as hdgx_schur_uq / hdgx_schur_u: the

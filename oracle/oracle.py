@@ -523,3 +523,13 @@ def getq(master, app, dgnodes, bf, UDG, UHe, SH=None, fc_q=1.0):
     if SH is not None:
         Q = Q + np.asarray(SH)[:, ncu:, :] / fc_q
     return Q
+
+
+def residual(master, app, dgnodes, bf, UDG, UHe, SH=None):
+    """kernel/cuda_residual.m on the CPU: q = getq(u, uh, SH, fc_q), then the oracle's element u
+    residual Ru (volint + faceint) at that q."""
+    ncu = app.ncu
+    U = np.array(UDG, dtype=np.float64, copy=True)
+    U[:, ncu:, :] = getq(master, app, dgnodes, bf, U, UHe, SH, app.fc_q)
+    sh = np.zeros_like(U) if SH is None else SH
+    return hdg_elemental(master, app, dgnodes, bf, U, UHe, sh, intermediates=True)["Ru"]

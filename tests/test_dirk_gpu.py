@@ -91,3 +91,24 @@ def test_getq_matches_oracle(oracle, name, kw):
         assert int(st.numpy().max()) == 0
         err = relerr(Q.numpy(), ref)
         assert err < bound, f"{name} fc_q={fc_q} relerr {err:.3e} > {bound:.3e}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw,tdep", [("c1", dict(n=4, porder=2), 0), ("c2", dict(n=4, porder=3), 0),
+                                          ("c2", dict(n=4, porder=3), 1), ("c4", dict(n=2, porder=2), 0)])
+def test_residual_matches_oracle(oracle, name, kw, tdep):
+    """hdgx_residual (kernel/cuda_residual.m: Ru at q = getq(u, uh)) against the oracle's
+    restatement.  Ru sums O(1) volume and face terms of a smooth state, so the bound is, as for
+    getq and DUDG, max(1e-12, 10 x the oracle's own change under one-ulp input perturbations)."""
+    from hdg_b200.elemental import residual
+    P = configs.by_name(name, **kw)
+    app, SH = (_tdep(P, 7.3) if tdep else (P.app, None))
+    rng = np.random.default_rng(21)
+    jit = lambda x: x * (1.0 + 2.2e-16 * rng.standard_normal(x.shape))
+    ref = oracle.residual(P.master, app, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), SH)
+    ref1 = oracle.residual(P.master, app, jit(P.mesh.dgnodes), P.mesh.bf, jit(P.UDG), jit(P.uh_elem()), SH)
+    bound = max(1e-12, 10.0 * relerr(ref1, ref))
+    Ru, st = residual(P.master, app, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), SH)
+    assert int(st.numpy().max()) == 0
+    err = relerr(Ru.numpy(), ref)
+    assert err < bound, f"{name} tdep={tdep} relerr {err:.3e} > {bound:.3e}"

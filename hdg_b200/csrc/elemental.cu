@@ -388,8 +388,12 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             continue;
         }
         if (P.RU) {
-            // cuda_residual.m:3-4: q from getq, then the u residual is evaluated at that q
-            for (int i = tid; i < NPV * NCU * ND; i += NT) s_udg[NPV * NCU + i] = s_MiRq[i];
+            // cuda_residual.m:3-4: q from getq, then the u residual is evaluated at that q; Rq is
+            // zero at that q, so Mi Rq (and its Gauss-point values below) are set to exact zeros
+            for (int i = tid; i < NPV * NCU * ND; i += NT) {
+                s_udg[NPV * NCU + i] = s_MiRq[i];
+                s_MiRq[i] = 0.0;
+            }
             __syncthreads();
             for (int i = tid; i < NGV * NCU * ND; i += NT) {
                 const int g = i % NGV, c = NCU + i / NGV;
@@ -595,9 +599,8 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                 for (int id = 0; id < ND; id++) {
                     double w = x_wrk[g + NGV * (id + ND * a)];
                     if constexpr (VISC) {
-                        if (!P.RU)                     // residual mode: Rq = 0 at q = getq
-                            for (int bd = 0; bd < NCU * ND; bd++)
-                                w -= x_wrl[g + NGV * (id + ND * (a + NCU * (NCU + bd)))] * x_Zr[g + NGV * bd];
+                        for (int bd = 0; bd < NCU * ND; bd++)
+                            w -= x_wrl[g + NGV * (id + ND * (a + NCU * (NCU + bd)))] * x_Zr[g + NGV * bd];
                     }
                     v += t_vg[r + NPV * (g + NGV * (id + 1))] * w;
                 }
@@ -609,9 +612,8 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     const int gg = g + NGF * j;
                     double w = -x_FH[gg + NGT * a];
                     if constexpr (VISC) {
-                        if (!P.RU)
-                            for (int bd = 0; bd < NCU * ND; bd++)
-                                w -= x_FHu[gg + NGT * (a + NCU * (NCU + bd))] * x_ZFr[gg + NGT * bd];
+                        for (int bd = 0; bd < NCU * ND; bd++)
+                            w -= x_FHu[gg + NGT * (a + NCU * (NCU + bd))] * x_ZFr[gg + NGT * bd];
                     }
                     v += t_fg[m + NPF * g] * w;
                 }

@@ -18,6 +18,7 @@
 // H is face-block diagonal and is added directly.  Results equal the reference's up to
 // floating-point summation order.
 #include <cuda_runtime.h>
+#include <type_traits>
 #include <math.h>
 #include "hdgx_common.cuh"
 
@@ -834,11 +835,13 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         //   Xg  = X at the face Gauss points (shapft through perm), per face
         //   Y   = Gp Xg, per face Gauss point (GK applied without forming it)
         //   AE  = shapfg Y (+ the face-block-diagonal H), per face
-        {
+        // nco (components stored per row block) is a compile-time constant inside the tiles
+        auto tiles = [&](auto nco_c) {
+            constexpr int NCO = decltype(nco_c)::value;
             constexpr int T = L::TILE;
             constexpr int TMQ = NPV <= 6 ? NPV : (NPV + 1) / 2;
             double *yX = sm + L::y_X, *yXg = sm + L::y_Xg, *yY = sm + L::y_Y;
-            double *g_dd = P.DUDG_DUH + (size_t)e * NPV * P.nco * NH;   // [npv, nco, ncu, ndf]
+            double *g_dd = P.DUDG_DUH + (size_t)e * NPV * NCO * NH;     // [npv, nco, ncu, ndf]
             double *g_ae = P.AE + (size_t)e * NH * NH;
             for (int k0 = 0; k0 < NH; k0 += T) {
                 const int nt = (NH - k0) < T ? (NH - k0) : T;
@@ -846,7 +849,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     const int ru = i % NU, t = i / NU;
                     const double v = s_R[NU * (1 + k0 + t) + ru];
                     yX[ru + NQ * t] = v;
-                    g_dd[(size_t)NPV * P.nco * (k0 + t) + ru] = v;
+                    g_dd[(size_t)NPV * NCO * (k0 + t) + ru] = v;
                 }
                 // q rows r + NPV (NCU + a + NCU d) of column k = k0 + t, batch d, n = (a, t)
                 tile_gemm<ND, NPV, NCU * T, NPV, TMQ, 2, NT>(
@@ -862,7 +865,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                         if (a == k % NCU) v -= s_MiE[r + NPV * (k / NCU + NDF * d)];
                         const int row = r + NPV * (NCU + a + NCU * d);
                         yX[row + NQ * t] = v;
-                        if (P.nco == NC) g_dd[(size_t)NQ * k + row] = v;
+                        if constexpr (NCO == NC) g_dd[(size_t)NQ * k + row] = v;
                     });
                 __syncthreads();
                 // Xg(gg, c, t) = sum_m shapft(g, m) X(perm(m, j), c, t), batch j, n = (c, t)
@@ -897,7 +900,9 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     });
                 __syncthreads();
             }
-        }
+        };
+        if (P.nco == NC) tiles(std::integral_constant<int, NC>{});
+        else tiles(std::integral_constant<int, NCU>{});
         if (tid == 0 && P.status) P.status[e] = *s_bad;
         __syncthreads();
     }

@@ -10,6 +10,7 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
                      double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed,
                      int grid, double *QDG = nullptr, double *RU = nullptr);
 cudaMemPool_t device_pool();
+int elemental_check_master(const hdgx_master *m);
 int schur_adjoint_launch(int qform, int nd, int npv, int ncu, int nc, int ndf, int ne, const double *M,
                          const double *C, const double *E, const double *BD, const double *F, const double *GK,
                          const double *H, const double *Rq, const double *Ru, const double *Rh, double *DUDG,
@@ -36,7 +37,8 @@ const char *hdgx_status_str(int code) {
         case 0: return "ok";
         case -1: return "invalid argument (null pointer or negative size)";
         case -2: return "inconsistent dimensions (nd, ncu, nc, npv, npf, nfe)";
-        case -3: return "unsupported element size (shared-memory plan does not fit)";
+        case -3: return "unsupported element: (nd, porder) not compiled, or master tables (npv, npf, ngv, ngf) "
+                        "other than those of quadrature order pgauss = 2 porder";
         case -4: return "too many boundary indices";
         case -5: return "system too large for the allocation-free scratch (hdgx_gmres_bilu0_noalloc: 16 MiB)";
         case -10: return "cudaFuncSetAttribute failed";
@@ -85,7 +87,7 @@ int check_elemental(const hdgx_master *master, const hdgx_app *app, int ne, cons
         return -2;
     if (app->localsolve != 1 || (app->getdqdg != 0 && app->getdqdg != 1)) return -2;
     if (app->nbnd < 0 || app->nbnd > HDGX_MAX_BND) return -4;
-    return 0;
+    return hdgx::elemental_check_master(master);     // -3: tables of another (porder, pgauss)
 }
 
 // Side streams of the bucketed launch, per device, created on the first call.

@@ -5,6 +5,7 @@
 #include <utility>
 #include <vector>
 #include "hdgx_common.cuh"
+#include "trace_internal.cuh"
 
 namespace hdgx {
 __global__ void gather_uh_kernel(int, int, int, const int *, const double *, double *);
@@ -27,19 +28,6 @@ __global__ void bilu0_sched_sweep_kernel(int, int, int, const int *, const long 
                                          const double *, const double *, double *, int *);
 __global__ void sched_begin_kernel(int *);
 __global__ void backsub_kernel(int, int, int, int, const int *, const double *, const double *, const double *, double *);
-__global__ void dot_partial_kernel(size_t, const double *, const double *, double *);
-__global__ void dot_final_kernel(int, const double *, double *, int);
-__global__ void axpy_kernel(size_t, const double *, double, const double *, double *);
-__global__ void scale_div_kernel(size_t, const double *, const double *, double *);
-__global__ void sub_kernel(size_t, const double *, const double *, double *);
-__global__ void axpby_kernel(size_t, double, const double *, double, double *);
-struct GmresState {
-    double *H, *cs, *sn, *g, *y;
-    double *scal;
-};
-__global__ void givens_kernel(GmresState, int, int);
-__global__ void hess_solve_kernel(GmresState, int, int);
-__global__ void gmres_init_kernel(GmresState, int);
 
 template <int BS>
 __global__ void bilu0_fwd_bs_kernel(const int *, int, const long long *, const int *, const int *, const double *,
@@ -50,14 +38,8 @@ __global__ void bilu0_bwd_bs_kernel(const int *, int, const long long *, const i
 template <int BS>
 __global__ void bsr_matvec_bs_kernel(int, const long long *, const int *, const double *, const double *, double *);
 
-// SM count of the current device (queried each time: host threads of a server may call in
-// concurrently and on different devices)
-static int sm_count() {
-    int d = 0, n = 0;
-    cudaGetDevice(&d);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d);
-    return n > 0 ? n : 1;
-}
+// SM count of the current device (cached per device ordinal)
+static int sm_count() { return sm_count_of(current_device()); }
 static unsigned grid_for(size_t n, int threads) {
     size_t g = (n + threads - 1) / threads;
     size_t cap = (size_t)sm_count() * 8;
@@ -72,7 +54,7 @@ static int launched() {
 
 static size_t bilu_smem(int bs) { return sizeof(double) * (4 * (size_t)bs * bs + 200 + 4 + 1); }
 
-static int matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *y, cudaStream_t st) {
+int trace_matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *y, cudaStream_t st) {
     const int threads = 256;
     const unsigned grid = grid_for((size_t)A->nf * 32, threads);
     switch (A->bs) {
@@ -113,7 +95,7 @@ static int resident_grid(const void *kern, int threads, size_t smem, int cap) {
     return g < cap ? g : cap;
 }
 
-static int bilu0_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *y, double *v, cudaStream_t st) {
+int trace_bilu0_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *y, double *v, cudaStream_t st) {
     const int threads = 256, warps = threads / 32;
     if (A->ncolors == 0) {
         if (!A->sched) return -1;
@@ -202,7 +184,7 @@ int hdgx_globalassembly(const hdgx_bsr *A, const hdgx_assembly_map *map, int ncu
 
 int hdgx_matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *y, hdgx_stream_t stream) {
     if (!A || !Hg || !x || !y) return -1;
-    return matvec(A, Hg, x, y, (cudaStream_t)stream);
+    return trace_matvec(A, Hg, x, y, (cudaStream_t)stream);
 }
 
 int hdgx_bilu0_factor(const hdgx_bsr *A, double *Mg, int *status, hdgx_stream_t stream) {
@@ -235,7 +217,7 @@ int hdgx_bilu0_factor(const hdgx_bsr *A, double *Mg, int *status, hdgx_stream_t 
 
 int hdgx_bilu0_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *v, double *work, hdgx_stream_t stream) {
     if (!A || !Mg || !x || !v || !work) return -1;
-    return bilu0_apply(A, Mg, x, work, v, (cudaStream_t)stream);
+    return trace_bilu0_apply(A, Mg, x, work, v, (cudaStream_t)stream);
 }
 
 int hdgx_backsub(int npv, int nc, int ncu, int ndf, int ne, const int *elcon, const double *DUDG,
@@ -267,19 +249,15 @@ size_t hdgx_gmres_workspace_bytes(const hdgx_bsr *A, int restart) {
     return sizeof(double) * (N * (m + 1) + 3 * N + (m + 1) * m + 4 * (m + 1) + 8 + 2048 + 2) + 256;
 }
 
-int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, const double *b, double *x, int restart,
-                     double tol, int maxit, int *iters, int *flag, double *relres, double *history, void *workspace,
-                     hdgx_stream_t stream) {
-    if (!A || !Hg || !Mg || !b || !x || restart < 1 || maxit < 1) return -1;
-    cudaStream_t st = (cudaStream_t)stream;
+}  // extern "C"
+
+namespace hdgx {
+
+int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const double *b, double *x, int restart,
+                    double tol, int maxit, int *iters, int *flag, double *relres, double *history, void *mem,
+                    cudaStream_t st) {
     const size_t N = (size_t)A->bs * A->nf;
     const int m = restart;
-    void *mem = workspace;
-    bool own = false;
-    if (!mem) {
-        if (cudaMallocAsync(&mem, hdgx_gmres_workspace_bytes(A, restart), st) != cudaSuccess) return -13;
-        own = true;
-    }
     double *V = (double *)mem;
     double *pb = V + N * (m + 1), *t = pb + N, *w2 = t + N;
     GmresState gs;
@@ -298,19 +276,25 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
     double h_scal[2] = {0.0, 0.0};
     double *h_nrmb = h_scal, *h_res = h_scal + 1;
     int rc = 0;
+    // a failed launch or copy ends the solve at the next synchronisation: no further work is queued
+    auto synced = [&]() {
+        const cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess && !rc) rc = -1000 - (int)e;
+        return rc == 0;
+    };
     // pb = P^{-1} b, nrmb = |pb|
-    rc |= bilu0_apply(A, Mg, b, t, pb, st);
+    if (int r = trace_bilu0_apply(A, Mg, b, t, pb, st)) rc = r;
     dot(N, pb, pb, gs.scal + 2, part, 1, st);
     cudaMemcpyAsync(h_nrmb, gs.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
+    synced();
     const double nrmb = *h_nrmb;
     int iter = 0, fl = 2;
     double res_rel = 0.0;
-    if (!(nrmb > 0.0)) { fl = 0; res_rel = 0.0; }
+    if (!(nrmb > 0.0) || rc) { fl = rc ? 3 : 0; res_rel = 0.0; }
     while (fl == 2) {
         // r = pb - P^{-1} A x -> V[:,0] = r / beta
-        rc |= matvec(A, Hg, x, t, st);
-        rc |= bilu0_apply(A, Mg, t, w2, V, st);
+        if (int r = trace_matvec(A, Hg, x, t, st)) rc = rc ? rc : r;
+        if (int r = trace_bilu0_apply(A, Mg, t, w2, V, st)) rc = rc ? rc : r;
         sub_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, pb, V, V);
         dot(N, V, V, gs.scal + 0, part, 1, st);
         scale_div_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, gs.scal + 0, V, V);
@@ -319,8 +303,8 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
         bool stop = false;
         for (int j = 0; j < m; j++) {
             double *vj = V + N * j, *w = V + N * (j + 1);
-            rc |= matvec(A, Hg, vj, t, st);
-            rc |= bilu0_apply(A, Mg, t, w2, w, st);
+            if (int r = trace_matvec(A, Hg, vj, t, st)) rc = rc ? rc : r;
+            if (int r = trace_bilu0_apply(A, Mg, t, w2, w, st)) rc = rc ? rc : r;
             double *hc = gs.H + (size_t)(m + 1) * j;
             if (!mgs_fused(N, j + 1, V, w, hc, part, bar, bar_err, st)) {
                 for (int i = 0; i <= j; i++) {        // modified Gram-Schmidt (gmres_bilu0.m:59-63)
@@ -332,7 +316,7 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
             }
             givens_kernel<<<1, 1, 0, st>>>(gs, m, j);
             cudaMemcpyAsync(h_res, gs.scal + 1, sizeof(double), cudaMemcpyDeviceToHost, st);
-            cudaStreamSynchronize(st);
+            if (!synced()) { fl = 3; stop = true; break; }
             res_rel = *h_res / nrmb;
             if (history && iter < maxit) history[iter] = res_rel;
             iter++;
@@ -341,28 +325,50 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
             if (res_rel <= tol) { fl = 0; stop = true; break; }
             if (iter >= maxit) { fl = 1; stop = true; break; }
         }
+        if (rc) break;
         hess_solve_kernel<<<1, 1, 0, st>>>(gs, m, jdone);
         // x += V y  (y on the device; one axpy per basis vector)
         for (int i = 0; i < jdone; i++) axpy_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, gs.y + i, 1.0, V + N * i, x);
         if (stop) break;
     }
-    cudaStreamSynchronize(st);
+    synced();
     if (iters) *iters = iter;
     if (flag) *flag = fl;
     if (relres) *relres = res_rel;
     int mgs_err = 0;
     cudaMemcpyAsync(&mgs_err, bar_err, sizeof(int), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
+    synced();
     int sched_err = 0;
     if (A->ncolors == 0 && A->sched) {
-        cudaMemcpy(&sched_err, A->sched + 2, sizeof(int), cudaMemcpyDeviceToHost);
-        if (sched_err) cudaMemset(A->sched + 2, 0, sizeof(int));
+        cudaMemcpyAsync(&sched_err, A->sched + 2, sizeof(int), cudaMemcpyDeviceToHost, st);
+        synced();
+        if (sched_err) cudaMemsetAsync(A->sched + 2, 0, sizeof(int), st);
     }
-    if (own) cudaFreeAsync(mem, st);
+    if (rc) return rc;
     if (cudaGetLastError() != cudaSuccess) return -12;
     if (sched_err) return -14;
     if (mgs_err) return -15;
-    return rc ? -12 : 0;
+    return 0;
+}
+
+}  // namespace hdgx
+
+extern "C" {
+
+int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, const double *b, double *x, int restart,
+                     double tol, int maxit, int *iters, int *flag, double *relres, double *history, void *workspace,
+                     hdgx_stream_t stream) {
+    if (!A || !Hg || !Mg || !b || !x || restart < 1 || maxit < 1) return -1;
+    cudaStream_t st = (cudaStream_t)stream;
+    void *mem = workspace;
+    bool own = false;
+    if (!mem) {
+        if (cudaMallocAsync(&mem, hdgx_gmres_workspace_bytes(A, restart), st) != cudaSuccess) return -13;
+        own = true;
+    }
+    const int rc = gmres_bilu0_run(A, Hg, Mg, b, x, restart, tol, maxit, iters, flag, relres, history, mem, st);
+    if (own) cudaFreeAsync(mem, st);
+    return rc;
 }
 
 }  // extern "C"

@@ -13,20 +13,9 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include "hdgx_common.cuh"
+#include "trace_internal.cuh"
 
 namespace hdgx {
-__global__ void dot_partial_kernel(size_t, const double *, const double *, double *);
-__global__ void dot_final_kernel(int, const double *, double *, int);
-__global__ void axpy_kernel(size_t, const double *, double, const double *, double *);
-__global__ void scale_div_kernel(size_t, const double *, const double *, double *);
-__global__ void sub_kernel(size_t, const double *, const double *, double *);
-struct GmresState {
-    double *H, *cs, *sn, *g, *y;
-    double *scal;
-};
-__global__ void givens_kernel(GmresState, int, int);
-__global__ void hess_solve_kernel(GmresState, int, int);
-__global__ void gmres_init_kernel(GmresState, int);
 
 // C(:, i) = A(:, :, i) B(:, i)   (arraymul.c:60-69); one thread per output row
 __global__ void batched_gemv_kernel(int rows, int cols, int nb, const double *__restrict__ A,

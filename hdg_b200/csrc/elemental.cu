@@ -919,11 +919,15 @@ static int launch_t(const ElemParams &p, cudaStream_t st, int grid_req) {
     auto kern = elemental_kernel<D, VISC, MIXED, NT>;
     cudaError_t err = allow_dynamic_smem((const void *)kern, smem);
     if (err != cudaSuccess) return -10;
-    int dev = 0, nsm = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
-    if (per_sm < 1) return -11;
+    // resident CTAs per SM of this instantiation, once per device
+    static std::atomic<int> per_sm_cache[kMaxDevices];
+    const int dev = current_device(), nsm = sm_count_of(dev);
+    int per_sm = per_sm_cache[dev < kMaxDevices ? dev : 0].load(std::memory_order_relaxed);
+    if (per_sm < 1) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem) != cudaSuccess) per_sm = 0;
+        if (per_sm < 1) return -11;
+        per_sm_cache[dev < kMaxDevices ? dev : 0].store(per_sm, std::memory_order_relaxed);
+    }
     int grid = grid_req > 0 ? grid_req : nsm * per_sm;     // default: one wave of resident CTAs
     if (grid > p.ne) grid = p.ne;
     if (grid < 1) return 0;
@@ -936,6 +940,41 @@ template <class D>
 static int launch_v(const ElemParams &p, bool visc, bool mixed, cudaStream_t st, int grid) {
     if (mixed) return visc ? launch_t<D, true, true>(p, st, grid) : launch_t<D, false, true>(p, st, grid);
     return visc ? launch_t<D, true, false>(p, st, grid) : launch_t<D, false, false>(p, st, grid);
+}
+
+// The compiled element shapes, keyed by (nd, porder).  Their Gauss point counts are those of
+// the drivers' quadrature order pgauss = 2 porder (mkmaster(mesh, 2*porder), e.g.
+// problem/euler/euler_trefftz.m:55); f(Dims{}) is called for the match, -3 returned otherwise.
+template <class F>
+static int with_dims(int nd, int po, F &&f) {
+    if (nd == 2) {
+        switch (po) {
+            case 1: return f(Dims<2, 3, 2, 3, 2>{});
+            case 2: return f(Dims<2, 6, 3, 6, 3>{});
+            case 3: return f(Dims<2, 10, 4, 12, 4>{});
+            case 4: return f(Dims<2, 15, 5, 16, 5>{});
+        }
+    } else if (nd == 3) {
+        switch (po) {
+            case 1: return f(Dims<3, 4, 3, 4, 3>{});
+            case 2: return f(Dims<3, 10, 6, 11, 6>{});
+        }
+    }
+    return -3;
+}
+
+// 0 when the master's table sizes are those of the compiled kernel for its (nd, porder), -3
+// otherwise.  mkmaster(mesh, pgauss) (master/mkmaster.m:1) takes the quadrature order as a
+// free argument; a master built with pgauss != 2 porder has other ngv / ngf, and the kernel,
+// whose loops run over the compiled extents, would index its tables out of range.
+int elemental_check_master(const hdgx_master *m) {
+    if (!m) return -1;
+    return with_dims(m->nd, m->porder, [&](auto d) -> int {
+        using D = decltype(d);
+        const bool ok = m->npv == D::NPV && m->npf == D::NPF && m->ngv == D::NGV && m->ngf == D::NGF &&
+                        m->nfe == D::NFE;
+        return ok ? 0 : -3;
+    });
 }
 
 int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const double *dgnodes,
@@ -962,21 +1001,10 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
     p.RU = RU;
     p.nco = app->getdqdg ? app->nc : app->ncu;
     const bool visc = p.pc.rinv != 0.0;
-    const int nd = m->nd, po = m->porder;
-    if (nd == 2) {
-        switch (po) {
-            case 1: return launch_v<Dims<2, 3, 2, 3, 2>>(p, visc, mixed, st, grid);
-            case 2: return launch_v<Dims<2, 6, 3, 6, 3>>(p, visc, mixed, st, grid);
-            case 3: return launch_v<Dims<2, 10, 4, 12, 4>>(p, visc, mixed, st, grid);
-            case 4: return launch_v<Dims<2, 15, 5, 16, 5>>(p, visc, mixed, st, grid);
-        }
-    } else if (nd == 3) {
-        switch (po) {
-            case 1: return launch_v<Dims<3, 4, 3, 4, 3>>(p, visc, mixed, st, grid);
-            case 2: return launch_v<Dims<3, 10, 6, 11, 6>>(p, visc, mixed, st, grid);
-        }
-    }
-    return -3;
+    if (int rc = elemental_check_master(m)) return rc;   // nothing is launched for a foreign master
+    return with_dims(m->nd, m->porder, [&](auto d) -> int {
+        return launch_v<decltype(d)>(p, visc, mixed, st, grid);
+    });
 }
 
 }  // namespace hdgx

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "../../include/hdgx.h"
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -24,6 +25,25 @@ inline cudaError_t allow_dynamic_smem(const void *fn, size_t bytes) {
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e == cudaSuccess) g = bytes;
     return e;
+}
+
+// Device attributes that every launch needs, cached per device ordinal (host threads of a
+// server may launch concurrently and on different devices; the values never change for a
+// device within a process).
+constexpr int kMaxDevices = 64;
+inline int current_device() {
+    int dev = 0;
+    return cudaGetDevice(&dev) == cudaSuccess ? dev : 0;
+}
+inline int sm_count_of(int dev) {
+    static std::atomic<int> cache[kMaxDevices];
+    if (dev < 0 || dev >= kMaxDevices) dev = 0;
+    int n = cache[dev].load(std::memory_order_relaxed);
+    if (n <= 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return 1;
+        cache[dev].store(n, std::memory_order_relaxed);
+    }
+    return n;
 }
 }  // namespace hdgx
 

@@ -19,6 +19,8 @@
 
 namespace hdgx {
 
+int elemental_check_master(const hdgx_master *m);
+
 // y = x0 + alpha * d   (the line-search update hdg_solve.m:146-147)
 __global__ void add_scaled_kernel(size_t n, const double *__restrict__ x0, double alpha, const double *__restrict__ d,
                                   double *__restrict__ y) {
@@ -241,6 +243,7 @@ extern "C" int hdgx_solve(const hdgx_master *m, const hdgx_app *app, const hdgx_
     const int ne = mesh->ne, nf = mesh->nf;
     if (ne < 1 || nf < 1 || opts->restart < 1 || opts->maxiter < 0 || opts->gmres_maxit < 1) return -1;
     if (app->getdqdg != 1) return -2;    // the native loop keeps q in the local solve (getdqdg = 1)
+    if (int rc = hdgx::elemental_check_master(m)) return rc;   // before any set-up or allocation
     if (opts->ordering != 0 && opts->ordering != 1) return -1;
     cudaStream_t st = (cudaStream_t)stream;
     const int npv = m->npv, npf = m->npf, nfe = m->nfe, ncu = app->ncu, nc = app->nc;

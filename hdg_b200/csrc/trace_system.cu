@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include "hdgx_common.cuh"
+#include "trace_internal.cuh"
 
 namespace hdgx {
 
@@ -339,10 +340,6 @@ __global__ void axpby_kernel(size_t n, double a, const double *__restrict__ x, d
 }
 
 // GMRES state on the device: H[(m+1) x m] column-major, cs, sn, g[m+1], scalars.
-struct GmresState {
-    double *H, *cs, *sn, *g, *y;
-    double *scal;      // [0] beta, [1] |g_{j+1}|, [2] scratch norm
-};
 
 // Apply the previous rotations to column j of H, form the new one, update g.  One thread.
 __global__ void givens_kernel(GmresState s, int m, int j) {
@@ -423,11 +420,16 @@ __global__ void __launch_bounds__(NT) block_norms_kernel(int bs, int nf, const l
 template __global__ void block_norms_kernel<256>(int, int, const long long *, const double *, double *);
 
 // Flag-scheduled sweeps and factorisation in an arbitrary sequential order.  sched[] layout:
-// [0] epoch, [1] work counter, [2] error flag, [3] spare, [4 + i] ready flag of row i.
-// Rows are taken in order through the counter, so a row only waits for rows taken before it
-// by CTAs / warps that are already running; every wait is bounded (HDGX_SPIN_LIMIT polls),
+// [0] epoch, [1] work counter, [2] error flag, [3] poll limit of every wait (0: HDGX_SPIN_LIMIT),
+// [4 + i] ready flag of row i.  Rows are taken in order through the counter, so a row only waits
+// for rows taken before it by CTAs / warps that are already running; every wait is bounded,
 // after which the error flag is raised and the row proceeds.
 #define HDGX_SPIN_LIMIT (1 << 22)
+
+__device__ __forceinline__ int poll_limit(const int *sched) {
+    const int l = sched[3];
+    return l > 0 ? l : HDGX_SPIN_LIMIT;
+}
 
 // ------------------------------------------------------------- fused Gram-Schmidt step
 // Blocks of one cooperative launch meet here.  Thread 0 of each block arrives on a counter; the
@@ -512,10 +514,10 @@ __device__ __forceinline__ int load_acquire(const int *p) {
     return v;
 }
 
-__device__ __forceinline__ void wait_flag(const int *flag, int epoch, int *err) {
+__device__ __forceinline__ void wait_flag(const int *flag, int epoch, int *err, int limit) {
     int n = 0;
     while (load_acquire(flag) != epoch) {
-        if (++n > HDGX_SPIN_LIMIT) { atomicExch(err, 1); break; }
+        if (++n > limit) { atomicExch(err, 1); break; }
         if (n > 64) __nanosleep(64);
     }
 }
@@ -542,7 +544,7 @@ __global__ void __launch_bounds__(NT) bilu0_sched_factor_kernel(int bs, int nf, 
     unsigned long long *slot = reinterpret_cast<unsigned long long *>(sm + 4 * b2 + 200);
     int *bad = reinterpret_cast<int *>(slot + 4);
     const int tid = threadIdx.x;
-    const int epoch = sched[0];
+    const int epoch = sched[0], limit = poll_limit(sched);
     int *flags = sched + 4, *err = sched + 2;
     for (;;) {
         if (tid == 0) {
@@ -565,7 +567,7 @@ __global__ void __launch_bounds__(NT) bilu0_sched_factor_kernel(int bs, int nf, 
             }
             *nl = n;
             *bad = 0;
-            for (int s = 0; s < n; s++) wait_flag(flags + (colind[lower[s]] - 1), epoch, err);
+            for (int s = 0; s < n; s++) wait_flag(flags + (colind[lower[s]] - 1), epoch, err, limit);
         }
         __syncthreads();
         for (int t = tid; t < b2; t += NT) Aii[t] = Mg[(size_t)b2 * k0 + t];
@@ -629,7 +631,7 @@ __global__ void bilu0_sched_sweep_kernel(int bs, int nf, int dir, const int *__r
     extern __shared__ double sh[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     double *t = sh + w * bs;
-    const int epoch = sched[0];
+    const int epoch = sched[0], limit = poll_limit(sched);
     int *flags = sched + 4, *err = sched + 2;
     for (;;) {
         int q = 0;
@@ -641,7 +643,7 @@ __global__ void bilu0_sched_sweep_kernel(int bs, int nf, int dir, const int *__r
         if (lane == 0)
             for (long long k = k0 + 1; k < k1; k++) {
                 const int j = colind[k] - 1;
-                if (dir ? (pos[j] > pi) : (pos[j] < pi)) wait_flag(flags + j, epoch, err);
+                if (dir ? (pos[j] > pi) : (pos[j] < pi)) wait_flag(flags + j, epoch, err, limit);
             }
         __syncwarp();
         for (int r = lane; r < bs; r += 32) {

@@ -87,7 +87,11 @@ int hdgx_status_count(const int *status, int n, hdgx_stream_t stream);
  * Outputs: AE[ncu,ndf,ncu,ndf,ne], FE[ncu,ndf,ne], DUDG[npv,nco,ne], DUDG_DUH[npv,nco,ncu,ndf,ne]
  *          (ndf = npf*nfe; nco = nc, or ncu when app->getdqdg = 0: the u rows only, as
  *          hdg_elemental.m:20-26 sizes them), status[ne] (may be NULL).
- * Supported (nd, porder): 2D 1..4, 3D 1..2; returns -3 otherwise. */
+ * Supported (nd, porder): 2D 1..4, 3D 1..2, with the drivers' quadrature order pgauss = 2 porder
+ * (mkmaster(mesh, 2*porder)); returns -3, before anything is launched, for any other (nd, porder)
+ * and for a master whose npv, npf, ngv or ngf differ from that element's (e.g. one built by
+ * mkmaster(mesh, pgauss) with pgauss != 2 porder).  hdgx_elemental_mixed, _host, _buckets,
+ * hdgx_getq, hdgx_residual and hdgx_solve apply the same check. */
 int hdgx_elemental(const hdgx_master *master, const hdgx_app *app, int ne,
                    const double *dgnodes, const int *bf, const double *UDG, const double *UH,
                    const double *SH, double *AE, double *FE, double *DUDG, double *DUDG_DUH,
@@ -214,7 +218,10 @@ typedef struct {
     int *sched;                /* ncolors == 0 only: device workspace of 4 + nf ints, zeroed once by
                                   the caller.  Rows are then eliminated one after another in the
                                   order color_rows (e.g. the MDF order of computeMDFordering.m), with
-                                  flag-synchronised (not level-synchronised) parallel sweeps. */
+                                  flag-synchronised (not level-synchronised) parallel sweeps.  Every
+                                  wait for a row's flag is bounded: sched[3] is the poll limit (0, as
+                                  zeroed: 2^22 polls); a wait that runs out sets sched[2], the row goes
+                                  on, and hdgx_gmres_bilu0 returns -14 (and clears sched[2]). */
     const int *sweep_plan;     /* optional (NULL: one launch per colour in hdgx_bilu0_apply): the
                                   colours as levels of a sequential order, for single-launch sweeps.
                                   Device ints: [ncolors+1] colour offsets, then for every slot q of
@@ -276,16 +283,20 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
                      int restart, double tol, int maxit, int *iters, int *flag, double *relres,
                      double *history, void *workspace, hdgx_stream_t stream);
 
-/* Allocation-free variant of hdgx_gmres_bilu0 (same arguments minus the workspace; same
- * algorithm and results).  No counterpart in the reference: it exists for callers that may
- * not allocate device or pinned host memory at solve time (a plugin host whose allocator
- * owns every byte, a latency-critical serving loop, memory already reserved in arenas).
- * Its scratch is one 16 MiB array compiled into the library, held by every GPU that loads
- * the library until exit; systems needing more (hdgx_gmres_workspace_bytes > 16 MiB,
- * roughly N > 88,000 unknowns at restart 20) are rejected with status -5.  All calls share
- * that array and it keeps the last call's contents, so calls that overlap on the GPU race;
- * the first call on each device resolves the array's address and should come before any
- * stream capture. */
+/* Allocation-free variant of hdgx_gmres_bilu0 (same arguments minus the workspace; the same
+ * solver code and kernels, so the same results bit for bit, for every ordering hdgx_bsr
+ * describes: colours, single-launch level sweeps, or flag-scheduled sweeps with the caller's
+ * `sched` array).  No counterpart in the reference: it exists for callers that may not
+ * allocate device or pinned host memory at solve time (a plugin host whose allocator owns
+ * every byte, a latency-critical serving loop, memory already reserved in arenas).  Its
+ * scratch is one 16 MiB array compiled into the library, held by every GPU that loads the
+ * library until exit; systems needing more (hdgx_gmres_workspace_bytes > 16 MiB, roughly
+ * N > 88,000 unknowns at restart 20) are rejected with status -5 before any work is queued.
+ * All calls share that array and it keeps the last call's contents (each call clears what
+ * it uses first), so calls that overlap on the GPU race.  With CUDA's lazy module loading
+ * the first call on a device loads the module and with it the array, and resolves the
+ * array's address: make that first call (a warm-up solve) before any latency-critical region
+ * and before any stream capture. */
 int hdgx_gmres_bilu0_noalloc(const hdgx_bsr *A, const double *Hg, const double *Mg, const double *b,
                              double *x, int restart, double tol, int maxit, int *iters, int *flag,
                              double *relres, double *history, hdgx_stream_t stream);

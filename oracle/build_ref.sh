@@ -7,12 +7,12 @@
 #       OpenBLAS (MATLAB's BLAS ABI uses ptrdiff_t integers);
 #   libref_ns.so : application/FM/ns/{flux,fhat}_ns{2,3}d.c and
 #       application/FM/euler/{flux,fhat}_euler{2,3}d.c (generated point kernels).
-# Usage: oracle/build_ref.sh [reference-root]
+# Usage: oracle/build_ref.sh REFERENCE_ROOT   (or HDG_REFERENCE=REFERENCE_ROOT oracle/build_ref.sh)
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:-${HDG_REFERENCE:-}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
-[ -d "$REF/kernel" ] || { echo "reference tree not found at $REF; skipping"; exit 0; }
+[ -n "$REF" ] && [ -d "$REF/kernel" ] || { echo "reference tree not given or not found (${REF:-unset}); skipping"; exit 0; }
 mkdir -p "$OUT"
 OB=$(python -c 'import numpy, glob, os; print(glob.glob(os.path.join(os.path.dirname(numpy.__file__), os.pardir, "numpy.libs", "libscipy_openblas64_*.so"))[0])')
 OBDIR=$(dirname "$OB"); OBNAME=$(basename "$OB")

@@ -7,8 +7,10 @@ needs the *same* rule, digit for digit, so the numbers are carried over as data.
 This script parses the two MATLAB files and writes the tables for the degrees the
 hot path uses (triangles ``pgauss`` 1..8, tetrahedra ``pgauss`` 1..6).
 
-Usage: ``python hdg_b200/gen_quad_tables.py <path-to-reference-root>``
+Usage: ``python tests/golden/gen_quad_tables.py <path-to-reference-root>`` (or set ``HDG_REFERENCE``);
+it writes ``hdg_b200/_quad_tables.py``.
 """
+import os
 import re
 import sys
 from pathlib import Path
@@ -67,10 +69,12 @@ def main(ref_root):
             lines.append("    ),")
         lines.append("}")
         lines.append("")
-    dst = Path(__file__).with_name("_quad_tables.py")
+    dst = Path(__file__).resolve().parents[2] / "hdg_b200" / "_quad_tables.py"
     dst.write_text("\n".join(lines))
     print("wrote", dst, "tri degrees", sorted(tri), "tet degrees", sorted(tet))
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2 and not os.environ.get("HDG_REFERENCE"):
+        sys.exit("usage: gen_quad_tables.py REFERENCE_ROOT (or set HDG_REFERENCE)")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ["HDG_REFERENCE"])

@@ -18,6 +18,7 @@
 
 Usage: python tests/golden/make_golden.py [reference-root] [--only adjoint|binfile]
 """
+import os
 import sys
 from pathlib import Path
 
@@ -130,6 +131,14 @@ def main(ref):
         print(f.name, f.stat().st_size)
 
 
+def reference_root(args):
+    """The reference tree: the first argument, else $HDG_REFERENCE."""
+    root = args[0] if args else os.environ.get("HDG_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT [--only adjoint|binfile] (or set HDG_REFERENCE)")
+    return root
+
+
 if __name__ == "__main__":
     args = [x for x in sys.argv[1:] if not x.startswith("--only")]
     only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
@@ -137,6 +146,6 @@ if __name__ == "__main__":
     if only == "adjoint":
         adjoint_fixture()
     elif only == "binfile":
-        binfile_fixture(args[0] if args else "/root/reference")
+        binfile_fixture(reference_root(args))
     else:
-        main(args[0] if args else "/root/reference")
+        main(reference_root(args))

@@ -26,7 +26,7 @@ class HdgxApp(ct.Structure):
     _fields_ = [("nd", ct.c_int), ("ncu", ct.c_int), ("nc", ct.c_int), ("localsolve", ct.c_int),
                 ("getdqdg", ct.c_int), ("fc_q", ct.c_double), ("fc_u", ct.c_double), ("tdep", ct.c_int),
                 ("param", ct.c_double * 8), ("nbnd", ct.c_int), ("bcm", ct.c_int * HDGX_MAX_BND),
-                ("bcs", ct.c_double * (HDGX_MAX_BND * 5))]
+                ("bcs", ct.c_double * (HDGX_MAX_BND * 5)), ("fbou", ct.c_int)]
 
 
 class HdgxBsr(ct.Structure):

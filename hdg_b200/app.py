@@ -9,8 +9,14 @@ Physics is the compressible Navier--Stokes family of ``application/FM/ns`` with
 through the same (u,q) form with ``Re = inf`` (every viscous and heat-flux term carries a
 factor ``1/Re``, ``application/FM/ns/flux2d.m:30``), so the local block is ``npv*nc``.
 
-Boundary types (``bcm``) follow ``application/FM/ns/fbou.m``: 5 periodic (= fhat), 6
-Dirichlet ``fh = uh - uinf`` (``fbou.m:111-114``).
+Boundary types (``bcm``) are the case labels of the ``fbou.m`` of the app's physics folder
+(``fbou``): ``"ns"`` (``application/FM/ns/fbou.m``, ``fbou3d.m``) has 1 far field (Roe matrices
+of ``getan.m``), 2 adiabatic wall, 3 isothermal wall, 4 prescribed pressure, 5 periodic
+(= fhat), 6 Dirichlet ``fh = uh - uinf`` (``fbou.m:111-114``); ``"euler"``
+(``application/FM/euler/fbou.m``) has 1 far field (local Lax-Friedrichs), 2 slip wall, 3 and 4
+prescribed pressure, 5 density and energy extrapolated, and 6 Dirichlet as ``"ns"``.  Euler
+apps (``Re = inf``) take the ``"euler"`` family, as the reference's Euler drivers do
+(``problem/euler/euler_trefftz.m:3`` puts ``application/FM/euler`` on the path).
 
 The synthetic states stand in for the reference's driver scripts (``problem/euler/
 euler_trefftz.m:14-19`` freestream; seeded perturbations with a PCG64 generator).
@@ -21,6 +27,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+BC_FARFIELD = 1
+BC_WALL = 2
 BC_PERIODIC = 5
 BC_DIRICHLET = 6
 
@@ -38,6 +46,7 @@ class App:
     getdqdg: int = 1
     name: str = "ns"
     denseblock: int = 0               # hdg_solve.m:43-45: 1 = dense face-block GMRES (gmres.m)
+    fbou: str = "ns"                  # fbou.m family: "ns" (application/FM/ns) or "euler" (application/FM/euler)
 
     @property
     def ncu(self):
@@ -71,7 +80,8 @@ def make_app(nd, gam=1.4, re=np.inf, pr=0.72, minf=0.5, tau=2.0, nbnd=None, alph
     ui = freestream(nd, gam, minf, alpha)
     return App(nd=nd, param=np.array([gam, 0.0, re, pr, minf, tau], dtype=np.float64),
                bcm=np.full(nbnd, BC_DIRICHLET, dtype=np.int64),
-               bcs=np.tile(ui, (nbnd, 1)), name="euler" if not np.isfinite(re) else "ns")
+               bcs=np.tile(ui, (nbnd, 1)), name="euler" if not np.isfinite(re) else "ns",
+               fbou="euler" if not np.isfinite(re) else "ns")
 
 
 def _prim_to_cons(rho, vel, p, gam):

@@ -28,6 +28,7 @@ struct ElemParams {
     const double *shapvt, *shapvg, *shapmv, *shapft, *shapfg, *shapmf;
     const int *perm;
     PhysConst pc;
+    FbouConst fb;              // boundary-flux family and constants (fbou.m of the app's physics)
     double fc_q, fc_u;
     int tdep;                  // 1: time-dependent source s = SH_u - fc_u u (volint.m:180-221)
     int nbnd;
@@ -455,8 +456,9 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             const int bnd = s_bf[j] < 0;
             const int ib = bnd ? -s_bf[j] - 1 : 0;
             const int btype = bnd ? ((ib < P.nbnd) ? P.bcm[ib] : -1) : 0;
-            const bool dir = bnd && btype == 6;
-            if (bnd && btype != 5 && btype != 6) *s_bad = 3;
+            const bool dir = bnd && btype == 6;                        // ns/fbou.m:111-114, both families
+            const bool per = bnd && btype == 5 && P.fb.fam == 0;       // ns/fbou.m:109-110: fhat
+            const bool gen = bnd && !dir && !per;                      // the other fbou.m types
 #pragma unroll
             for (int a = 0; a < NCU; a++) {
                 double fn = 0.0, dfn = 0.0;
@@ -470,7 +472,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     const double fh = fn + P.pc.tau * (x_fu[gg + NGT * a] - x_fuh[gg + NGT * a]);
                     x_FH[gg + NGT * a] = jc * fh;
                     const double bh = dir ? (x_fuh[gg + NGT * a] - P.bcs[ib * 5 + a]) : fh;
-                    x_BH[gg + NGT * a] = jc * bh;
+                    if (!gen) x_BH[gg + NGT * a] = jc * bh;
                 }
                 if (sd < NCU) {
                     // dfhat/duh (seed on uh) and dfhat/du = tau I
@@ -478,11 +480,47 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     const double fhu = (a == sd ? P.pc.tau : 0.0);
                     x_FHh[gg + NGT * (a + NCU * sd)] = jc * fhh;
                     x_FHu[gg + NGT * (a + NCU * sd)] = jc * fhu;
-                    s_Hp[gg + NGT * (a + NCU * sd)] = jc * (dir ? (a == sd ? 1.0 : 0.0) : fhh);
-                    s_Gp[gg + NGT * (a + NCU * sd)] = jc * (dir ? 0.0 : fhu);
+                    if (!gen) {
+                        s_Hp[gg + NGT * (a + NCU * sd)] = jc * (dir ? (a == sd ? 1.0 : 0.0) : fhh);
+                        s_Gp[gg + NGT * (a + NCU * sd)] = jc * (dir ? 0.0 : fhu);
+                    }
                 } else {
                     x_FHu[gg + NGT * (a + NCU * sd)] = jc * dfn;
-                    s_Gp[gg + NGT * (a + NCU * sd)] = jc * (dir ? 0.0 : dfn);
+                    if (!gen) s_Gp[gg + NGT * (a + NCU * sd)] = jc * (dir ? 0.0 : dfn);
+                }
+            }
+            if (gen) {
+                // faceint.m:171-268: Rh, H and GK rows of this boundary face from fbou.m.  One pass
+                // seeded like the fhat above (uh for sd < NCU, q otherwise) and, for sd < NCU, one
+                // seeded on the interior u.
+                double nlp[ND];
+#pragma unroll
+                for (int d = 0; d < ND; d++) nlp[d] = x_nl[gg + NGT * d];
+                D1 uu[NCU], qq[NCU * ND], hh[NCU], fb[NCU];
+#pragma unroll
+                for (int c = 0; c < NCU; c++) {
+                    uu[c] = {x_fu[gg + NGT * c], 0.0};
+                    hh[c] = {x_fuh[gg + NGT * c], c == sd ? 1.0 : 0.0};
+                }
+#pragma unroll
+                for (int c = 0; c < NCU * ND; c++) qq[c] = {x_fu[gg + NGT * (NCU + c)], (NCU + c) == sd ? 1.0 : 0.0};
+                const double *ub = P.bcs + (ib < P.nbnd ? ib : 0) * 5;
+                if (!fbou_point<ND>(P.fb, P.pc, btype, ub, nlp, uu, qq, hh, fb)) *s_bad = 3;
+#pragma unroll
+                for (int a = 0; a < NCU; a++) {
+                    if (sd == 0) x_BH[gg + NGT * a] = jc * fb[a].v;
+                    if (sd < NCU) s_Hp[gg + NGT * (a + NCU * sd)] = jc * fb[a].d;
+                    else s_Gp[gg + NGT * (a + NCU * sd)] = jc * fb[a].d;
+                }
+                if (sd < NCU) {
+#pragma unroll
+                    for (int c = 0; c < NCU; c++) {
+                        uu[c].d = c == sd ? 1.0 : 0.0;
+                        hh[c].d = 0.0;
+                    }
+                    fbou_point<ND>(P.fb, P.pc, btype, ub, nlp, uu, qq, hh, fb);
+#pragma unroll
+                    for (int a = 0; a < NCU; a++) s_Gp[gg + NGT * (a + NCU * sd)] = jc * fb[a].d;
                 }
             }
         }
@@ -989,6 +1027,10 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
     p.pc.rinv = (re > 0.0 && isfinite(re)) ? 1.0 / re : 0.0;
     p.pc.kap = p.pc.rinv * gam / (pr * (gam - 1.0));
     p.pc.tau = app->param[5];
+    p.fb.fam = app->fbou;
+    p.fb.gam = gam;
+    p.fb.eps = app->param[1];
+    p.fb.m2 = app->param[4] * app->param[4];
     p.fc_q = app->fc_q;
     p.fc_u = app->fc_u;
     p.tdep = app->tdep;

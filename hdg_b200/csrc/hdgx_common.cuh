@@ -141,6 +141,166 @@ __device__ __forceinline__ void ns_flux(const PhysConst &pc, const D1 *u, const 
     }
 }
 
+// ------------------------------------------------------------ boundary fluxes (fbou)
+__device__ __forceinline__ D1 dsqrt(D1 a) {
+    const double r = sqrt(a.v);
+    return {r, a.d * 0.5 / r};
+}
+__device__ __forceinline__ D1 dabs(D1 a) { return a.v < 0.0 ? D1{-a.v, -a.d} : a; }   // sign(0) = 1
+__device__ __forceinline__ D1 dscale(D1 a, double s) { return {a.v * s, a.d * s}; }
+
+// Constants of the boundary fluxes: family (0: application/FM/ns/fbou.m and fbou3d.m,
+// 1: application/FM/euler/fbou.m), gam, the entropy-fix width eps = param[1], Minf^2.
+struct FbouConst {
+    int fam;
+    double gam, eps, m2;
+};
+
+// y = A x for the Roe matrices of getan.m at the state m (absolute = false: the normal flux
+// Jacobian A_n; true: |A_n|, with |l| replaced by (|l|^2/(eps c) + eps c)/2 where |l| < eps c).
+// A = l3 I + r1 w1' + r2 w2' (r1 = [1, v, h], r2 = [0, n, un], w1 = (s1-l3) gam1/c^2 P + s2/c N,
+// w2 = s2 gam1/c P + (s1-l3) N, P = [|v|^2/2, -v, 1], N = [-un, n, 0], l1,2,3 = un+c, un-c, un),
+// applied through its two rank-one terms instead of being formed.
+template <int ND>
+__device__ __forceinline__ void roe_apply(double gam, double eps, const double *nl, const D1 *m, bool absolute,
+                                          const D1 *x, D1 *y) {
+    constexpr int NCU = ND + 2;
+    const double gam1 = gam - 1.0;
+    const D1 r = m[0];
+    D1 v[ND], un = dc(0.0), af = dc(0.0);
+#pragma unroll
+    for (int i = 0; i < ND; i++) {
+        v[i] = m[1 + i] / r;
+        un = un + dscale(v[i], nl[i]);
+        af = af + dscale(v[i] * v[i], 0.5);
+    }
+    const D1 p = dscale(m[NCU - 1] - r * af, gam1);
+    const D1 c = dsqrt(dscale(p, gam) / r);
+    const D1 h = (m[NCU - 1] + p) / r;
+    D1 l[3] = {un + c, un - c, un};
+    if (absolute) {
+        const D1 ec = dscale(c, eps);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            l[i] = dabs(l[i]);
+            if (eps > 0.0 && l[i].v < ec.v) l[i] = dscale(l[i] * l[i] / ec + ec, 0.5);
+        }
+    }
+    const D1 s1 = dscale(l[0] + l[1], 0.5), s2 = dscale(l[0] - l[1], 0.5), d = s1 - l[2];
+    const D1 k1 = dscale(d, gam1) / (c * c), k2 = s2 / c, k3 = dscale(k2, gam1);
+    D1 Px = af * x[0] + x[NCU - 1], Nx = dc(0.0) - un * x[0];
+#pragma unroll
+    for (int i = 0; i < ND; i++) {
+        Px = Px - v[i] * x[1 + i];
+        Nx = Nx + dscale(x[1 + i], nl[i]);
+    }
+    const D1 w1 = k1 * Px + k2 * Nx, w2 = k3 * Px + d * Nx;
+    y[0] = l[2] * x[0] + w1;
+#pragma unroll
+    for (int i = 0; i < ND; i++) y[1 + i] = l[2] * x[1 + i] + v[i] * w1 + dscale(w2, nl[i]);
+    y[NCU - 1] = l[2] * x[NCU - 1] + h * w1 + un * w2;
+}
+
+// The boundary flux fh[NCU] of fbou.m at one face point, from the interior state u, its gradient
+// slots q, the trace uh and the boundary state ub = bcs(ib, :) (duals carry one derivative).
+//   ns    (ns/fbou.m, fbou3d.m)  1 far field (an + An)(u - uh) - (an - An)(ub - uh), an = A_n(uh),
+//         An = |A_n(uh)| (getan.m absolute 0 / 1); 2 adiabatic wall [u0 - uh0, -uh_m, fhat_E];
+//         3 isothermal wall [u0 - uh0, -uh_m, gam gam1 Minf^2 uh_E/uh0 - ub_E]; 4 prescribed pressure,
+//         the far-field form with ub replaced by [u0, u_m, p/gam1 + |u_m|^2/(2 u0)], p = (ub_E - 1/2) gam1;
+//   euler (euler/fbou.m)  1, 3, 4 the same forms with the local Lax-Friedrichs scalars an = |un| + c
+//         (eps > 0: ((|un| + c)^2/(eps c) + eps c)/2) and An = un - c of euler/getan.m at uh, p = ub_0
+//         for 3; 2 slip wall u - (u_m . n) n - uh; 5 [u0, ub_m, u_E] - uh.
+// Returns false for a type outside both lists.  Types 5 (ns: periodic = fhat) and 6 (Dirichlet)
+// are handled by the caller.
+template <int ND>
+__device__ __noinline__ bool fbou_point(const FbouConst &fc, const PhysConst &pc, int ib, const double *ub,
+                                        const double *nl, const D1 *u, const D1 *q, const D1 *uh, D1 *fh) {
+    constexpr int NCU = ND + 2;
+    const double gam1 = fc.gam - 1.0;
+    D1 ui[NCU];
+    const bool far = ib == 1 || ib == 4 || (fc.fam == 1 && ib == 3);
+    if (far) {
+        if (ib == 1) {
+#pragma unroll
+            for (int a = 0; a < NCU; a++) ui[a] = dc(ub[a]);
+        } else {
+            const double pb = (fc.fam == 1 && ib == 3) ? ub[0] : (ub[NCU - 1] - 0.5) * gam1;
+            D1 ke = dc(0.0);
+#pragma unroll
+            for (int i = 0; i < ND; i++) {
+                ui[1 + i] = u[1 + i];
+                ke = ke + u[1 + i] * u[1 + i] / u[0];
+            }
+            ui[0] = u[0];
+            ui[NCU - 1] = dc(pb / gam1) + dscale(ke, 0.5);
+        }
+        D1 a[NCU], b[NCU];
+#pragma unroll
+        for (int k = 0; k < NCU; k++) {
+            a[k] = u[k] - ui[k];                        // (an + An)(u - uh) - (an - An)(ui - uh)
+            b[k] = u[k] + ui[k] - dscale(uh[k], 2.0);   //   = an (u - ui) + An (u + ui - 2 uh)
+        }
+        if (fc.fam == 0) {
+            D1 y[NCU];
+            roe_apply<ND>(fc.gam, 0.0, nl, uh, false, a, fh);
+            roe_apply<ND>(fc.gam, fc.eps, nl, uh, true, b, y);
+#pragma unroll
+            for (int k = 0; k < NCU; k++) fh[k] = fh[k] + y[k];
+        } else {
+            const D1 r = uh[0];
+            D1 un = dc(0.0), af = dc(0.0);
+#pragma unroll
+            for (int i = 0; i < ND; i++) {
+                const D1 vi = uh[1 + i] / r;
+                un = un + dscale(vi, nl[i]);
+                af = af + dscale(vi * vi, 0.5);
+            }
+            const D1 c = dsqrt(dscale(dscale(uh[NCU - 1] - r * af, gam1), fc.gam) / r);
+            D1 an = dabs(un) + c;
+            if (fc.eps > 0.0) {
+                const D1 ec = dscale(c, fc.eps);
+                an = dscale(an * an / ec + ec, 0.5);
+            }
+            const D1 An = un - c;
+#pragma unroll
+            for (int k = 0; k < NCU; k++) fh[k] = an * a[k] + An * b[k];
+        }
+        return true;
+    }
+    if (fc.fam == 0 && (ib == 2 || ib == 3)) {
+        fh[0] = u[0] - uh[0];
+#pragma unroll
+        for (int i = 0; i < ND; i++) fh[1 + i] = dc(0.0) - uh[1 + i];
+        if (ib == 3) {
+            fh[NCU - 1] = dscale(uh[NCU - 1] / uh[0], fc.gam * gam1 * fc.m2) - dc(ub[NCU - 1]);
+        } else {
+            D1 f[NCU * ND];                                // the energy row of fhat at (uh, q)
+            ns_flux<ND>(pc, uh, q, f);
+            D1 e = dscale(u[NCU - 1] - uh[NCU - 1], pc.tau);
+#pragma unroll
+            for (int j = 0; j < ND; j++) e = e + dscale(f[(NCU - 1) + NCU * j], nl[j]);
+            fh[NCU - 1] = e;
+        }
+        return true;
+    }
+    if (fc.fam == 1 && ib == 2) {
+        D1 un = dc(0.0);
+#pragma unroll
+        for (int i = 0; i < ND; i++) un = un + dscale(u[1 + i], nl[i]);
+        fh[0] = u[0] - uh[0];
+#pragma unroll
+        for (int i = 0; i < ND; i++) fh[1 + i] = u[1 + i] - dscale(un, nl[i]) - uh[1 + i];
+        fh[NCU - 1] = u[NCU - 1] - uh[NCU - 1];
+        return true;
+    }
+    if (fc.fam == 1 && ib == 5) {
+#pragma unroll
+        for (int a = 0; a < NCU; a++) fh[a] = ((a == 0 || a == NCU - 1) ? u[a] : dc(ub[a])) - uh[a];
+        return true;
+    }
+    return false;
+}
+
 // --------------------------------------------------------------- block helpers
 template <int NT>
 __device__ __forceinline__ double block_reduce_max_abs(double v, double *red) {

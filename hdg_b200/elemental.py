@@ -98,6 +98,7 @@ def app_struct(app):
     for i, v in enumerate(np.asarray(app.param, dtype=np.float64)[:8]):
         s.param[i] = float(v)
     s.nbnd = nb
+    s.fbou = 1 if getattr(app, "fbou", "ns") == "euler" else 0
     for i in range(nb):
         s.bcm[i] = int(app.bcm[i])
         for a in range(app.ncu):

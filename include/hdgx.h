@@ -9,7 +9,7 @@
  * int status: 0 ok, < 0 bad argument / unsupported size / CUDA error (see hdgx_status_str).
  * Per-element numerical failures (zero or non-finite pivot) are reported through the
  * optional `status[ne]` array (0 ok, 1 singular mass matrix, 2 singular local system,
- * 3 unsupported boundary type) and counted in the return value of hdgx_status_count.
+ * 3 boundary type outside the app's fbou family) and counted in the return value of hdgx_status_count.
  *
  * Reference call surface each entry point replaces (paths relative to the reference tree):
  *   hdgx_elemental   kernel/hdg_elemental.m:1   [AE,FE,DUDG,DUDG_DUH] = hdg_elemental(master,app,dgnodes,bf,UDG,UH,SH)
@@ -70,8 +70,17 @@ typedef struct {
                                axisymmetry): source SH_u - fc_u u, Jacobian -fc_u on the u components */
     double param[8];        /* [gam, epslm, Re, Pr, Minf, tau]; Re = +inf gives Euler */
     int nbnd;               /* number of boundary indices (bf = -1..-nbnd) */
-    int bcm[HDGX_MAX_BND];  /* fbou type per boundary index: 5 periodic, 6 Dirichlet */
+    int bcm[HDGX_MAX_BND];  /* fbou type per boundary index (the case labels of the family's fbou.m) */
     double bcs[HDGX_MAX_BND * 5];  /* boundary state per index, row-major [nbnd][ncu] */
+    int fbou;               /* boundary-flux family, the app's physics folder (faceint.m:171-268 calls
+                               app.fbou of application/FM/<physics>):
+                               0 ns    (ns/fbou.m, fbou3d.m): 1 far field (Roe matrices of getan.m),
+                                       2 adiabatic wall, 3 isothermal wall, 4 prescribed pressure,
+                                       5 periodic (fhat), 6 Dirichlet uh - uinf;
+                               1 euler (euler/fbou.m): 1 far field (local Lax-Friedrichs scalars of
+                                       euler/getan.m), 2 slip wall, 3 and 4 prescribed pressure,
+                                       5 density and energy extrapolated, 6 Dirichlet as for ns.
+                               Other types give element status 3. */
 } hdgx_app;
 
 /* Library identity and error strings. */

@@ -27,7 +27,7 @@ class _Master(ct.Structure):
 class _App(ct.Structure):
     _fields_ = [("nd", ct.c_int), ("ncu", ct.c_int), ("nc", ct.c_int), ("localsolve", ct.c_int),
                 ("fc_q", ct.c_double), ("param", _dp), ("nbnd", ct.c_int), ("bcm", _ip), ("bcs", _dp),
-                ("fc_u", ct.c_double), ("tdep", ct.c_int)]
+                ("fc_u", ct.c_double), ("tdep", ct.c_int), ("fbou_family", ct.c_int)]
 
 
 def build():
@@ -66,7 +66,8 @@ def _keep(master, app):
                 F(master.shapvt), F(master.shapvg), F(master.shapmv), F(master.shapft),
                 F(master.shapfg), F(master.shapmf), I(master.perm))
     a = _App(app.nd, app.ncu, app.nc, app.localsolve, app.fc_q, F(app.param), len(app.bcm),
-             I(app.bcm), F(app.bcs), float(getattr(app, "fc_u", 0.0)), int(getattr(app, "tdep", 0)))
+             I(app.bcm), F(app.bcs), float(getattr(app, "fc_u", 0.0)), int(getattr(app, "tdep", 0)),
+             fbou_family(app))
     return m, a, keep
 
 
@@ -123,6 +124,30 @@ def flux_points(nd, param, udg):
     f = np.zeros((ng, ncu, nd), order="F"); fu = np.zeros((ng, ncu, nd, nc), order="F")
     L.orc_flux_points(nd, _p(_f(param)), ng, _p(_f(udg)), _p(f), _p(fu))
     return f, fu
+
+
+def fbou_family(app):
+    """0: application/FM/ns/fbou.m, 1: application/FM/euler/fbou.m (the app's physics folder)."""
+    return 1 if getattr(app, "fbou", "ns") == "euler" else 0
+
+
+def fbou_points(fam, nd, ib, uinf, param, nl, udg, uh):
+    """fbou of family fam (0 ns, 1 euler) at ng points: fh[ng,ncu], fh_udg[ng,ncu,nc], fh_uh[ng,ncu,ncu]."""
+    L = lib(); ng, nc = udg.shape; ncu = nd + 2
+    fh = np.zeros((ng, ncu), order="F"); fhu = np.zeros((ng, ncu, nc), order="F"); fhh = np.zeros((ng, ncu, ncu), order="F")
+    rc = L.orc_fbou_points(int(fam), nd, int(ib), _p(_f(uinf)), _p(_f(param)), ng, _p(_f(nl)), _p(_f(udg)), _p(_f(uh)),
+                           _p(fh), _p(fhu), _p(fhh))
+    if rc:
+        raise ValueError(f"boundary type {ib} of family {fam} is not restated")
+    return fh, fhu, fhh
+
+
+def getan_points(nd, param, absolute, nl, uh):
+    """Roe matrices of getan.m at ng trace states: An[ng,ncu,ncu], Anm[ng,ncu,ncu,ncu]."""
+    L = lib(); ng = uh.shape[0]; ncu = nd + 2
+    An = np.zeros((ng, ncu, ncu), order="F"); Anm = np.zeros((ng, ncu, ncu, ncu), order="F")
+    L.orc_getan_points(nd, _p(_f(param)), int(absolute), ng, _p(_f(nl)), _p(_f(uh)), _p(An), _p(Anm))
+    return An, Anm
 
 
 def fhat_points(nd, param, nl, udg, uh):

@@ -46,6 +46,7 @@ typedef struct {
     const double *bcs;             /* [nbnd, ncu] column-major */
     double fc_u;                   /* time-derivative coefficient (tdep = 1) */
     int tdep;                      /* 1: time-dependent source (volint.m:180-221) */
+    int fbou_family;               /* 0: application/FM/ns/fbou.m, 1: application/FM/euler/fbou.m */
 } orc_app;
 
 
@@ -409,7 +410,7 @@ static int element_blocks(const orc_master *ms, const orc_app *ap, const double 
                 for (int c = 0; c < nc; c++) tu[IX2(g, c, ngf)] = fug[IX2(gg, c, ngt)];
                 for (int a = 0; a < ncu; a++) th[IX2(g, a, ngf)] = fuh[IX2(gg, a, ngt)];
             }
-            if (orc_fbou(nd, ap->bcm[ibn], ui, ap->param, ngf, tn, tu, th, o1, o2, o3)) { rc = -3; continue; }
+            if (orc_fbou(ap->fbou_family, nd, ap->bcm[ibn], ui, ap->param, ngf, tn, tu, th, o1, o2, o3)) { rc = -3; continue; }
             for (int g = 0; g < ngf; g++) {
                 int gg = g + ngf * j;
                 for (int a = 0; a < ncu; a++) {
@@ -702,6 +703,25 @@ void orc_fhat_points(int nd, const double *param, int ng, const double *nl, cons
                      const double *uh, double *fh, double *fh_udg, double *fh_uh)
 { orc_fhat(nd, param, ng, nl, udg, uh, fh, fh_udg, fh_uh); }
 
-int orc_fbou_points(int nd, int ib, const double *uinf, const double *param, int ng, const double *nl,
+int orc_fbou_points(int fam, int nd, int ib, const double *uinf, const double *param, int ng, const double *nl,
                     const double *udg, const double *uh, double *fh, double *fh_udg, double *fh_uh)
-{ return orc_fbou(nd, ib, uinf, param, ng, nl, udg, uh, fh, fh_udg, fh_uh); }
+{ return orc_fbou(fam, nd, ib, uinf, param, ng, nl, udg, uh, fh, fh_udg, fh_uh); }
+
+/* An[ng, ncu, ncu] and its derivative Anm[ng, ncu, ncu, ncu] (last index: the uh component) of
+ * the Roe matrices at the states uh[ng, ncu] (getan.m absolute 0 or 1), for the fixture pins. */
+void orc_getan_points(int nd, const double *param, int absolute, int ng, const double *nl, const double *uh,
+                      double *An, double *Anm)
+{
+    const int ncu = nd + 2;
+    for (int g = 0; g < ng; g++) {
+        double n1[3];
+        odual m[5], A[25];
+        for (int d = 0; d < nd; d++) n1[d] = nl[g + ng * d];
+        for (int c = 0; c < ncu; c++) m[c] = od_var(uh[g + ng * c], c, ncu);
+        orc_getan_roe(nd, param, n1, m, absolute, ncu, A);
+        for (int k = 0; k < ncu * ncu; k++) {
+            An[g + ng * k] = A[k].v;
+            for (int c = 0; c < ncu; c++) Anm[g + ng * (k + ncu * ncu * c)] = A[k].d[c];
+        }
+    }
+}

@@ -13,10 +13,18 @@
                         (compiled the same way) on the blocks stored in ref_schur.npz; the u
                         form both on the D block alone and on the full BD / GK (nc > ncu).
 
+* ref_fbou.npz       -- outputs of the reference's generated boundary kernels
+                        application/FM/ns/fbou_ns{2,3}d.c (types 1 far field, 2 adiabatic wall,
+                        4 prescribed pressure) and application/FM/euler/fbou_euler{2,3}d.c (type 2
+                        slip wall), and of the Roe matrices of application/FM/getan.c (absolute 0
+                        and 1, with and without the entropy fix), on seeded random states; compiled
+                        into oracle/_ref by oracle/build_ref.sh.
+
 * binfile_format.json -- the header positions (ndims(k) = ...) and the fwrite sequence of the
                         single-process branch of util/writeBinaryFile.m, read from its source.
 
-Usage: python tests/golden/make_golden.py [reference-root] [--only adjoint|binfile]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT [--only adjoint|fbou|binfile]
+       (or set HDG_REFERENCE)
 """
 import os
 import sys
@@ -60,6 +68,60 @@ def adjoint_fixture():
             for k, v in zip(("DUDG", "DUDG_DUH", "AE", "FE"), outs):
                 adj[f"{tag}_{form}_{k}"] = v
     np.savez_compressed(OUT / "ref_schur_adjoint.npz", **adj)
+
+
+def fbou_states(nd, ng, seed):
+    """Seeded face-point states: interior udg[ng, nc], trace uh[ng, ncu], unit normals nl[ng, nd]
+    (every other normal nearly perpendicular to the velocity, so that |un| < eps c there and the
+    entropy fix of getan.m is exercised), a boundary state ub[ncu]."""
+    rng = np.random.default_rng(seed)
+    gam, minf = 1.4, 0.5
+    ncu = nd + 2
+    rho = 1.0 + 0.1 * rng.standard_normal(ng)
+    vel = 0.3 * rng.standard_normal((ng, nd)) + np.eye(nd)[0]
+    p = (1.0 + 0.05 * rng.standard_normal(ng)) / (gam * minf * minf)
+    u = np.column_stack([rho, rho[:, None] * vel, p / (gam - 1) + 0.5 * rho * (vel ** 2).sum(1)])
+    uh = u * (1.0 + 0.02 * rng.standard_normal(u.shape))
+    q = 0.1 * rng.standard_normal((ng, ncu * nd))
+    nl = rng.standard_normal((ng, nd))
+    vh = uh[:, 1:nd + 1] / uh[:, :1]
+    for g in range(0, ng, 2):                       # nearly tangential: un ~ 0
+        nl[g] -= (nl[g] @ vh[g]) / (vh[g] @ vh[g]) * vh[g]
+        nl[g] += 1e-3 * vh[g]
+    nl /= np.linalg.norm(nl, axis=1)[:, None]
+    ub = np.concatenate([[1.0], np.eye(nd)[0], [1.0 / (gam * (gam - 1) * minf * minf) + 0.5]])
+    return np.column_stack([u, q]), uh, nl, ub
+
+
+def fbou_fixture():
+    import ctypes as ct
+    from oracle import oracle as O
+    v = lambda a: a.ctypes.data_as(ct.c_void_p)
+    out = {}
+    for fam, types in (("ns", (1, 2, 4)), ("euler", (2,))):
+        L = ct.CDLL(str(O.HERE / "_ref" / f"libref_fbou_{fam}.so"))
+        for nd in (2, 3):
+            ncu, ng = nd + 2, 16
+            nc = ncu * (nd + 1)
+            udg, uh, nl, ub = (np.asfortranarray(a) for a in fbou_states(nd, ng, 7 + nd))
+            pg = np.zeros((ng, nd), order="F")
+            for eps in (0.0, 0.5):
+                param = np.array([1.4, eps, 1000.0, 0.72, 0.5, 2.0])
+                tag = f"{fam}{nd}d_e{int(eps > 0)}"
+                out[tag + "_udg"], out[tag + "_uh"], out[tag + "_nl"], out[tag + "_ub"] = udg, uh, nl, ub
+                out[tag + "_param"] = param
+                for ib in types:
+                    fh = np.zeros((ng, ncu), order="F"); fu = np.zeros((ng, ncu, nc), order="F")
+                    fhh = np.zeros((ng, ncu, ncu), order="F")
+                    L.ref_fbou(v(fh), v(fu), v(fhh), v(pg), v(udg), v(uh), v(nl), v(ub), v(param), ct.c_double(0.0),
+                               ib, ng, ncu, nc, nd, nd)
+                    out[f"{tag}_ib{ib}_fh"], out[f"{tag}_ib{ib}_fh_udg"], out[f"{tag}_ib{ib}_fh_uh"] = fh, fu, fhh
+                if fam == "ns":
+                    for ab in (0, 1):
+                        An = np.zeros((ng, ncu, ncu), order="F"); Anm = np.zeros((ng, ncu, ncu, ncu), order="F")
+                        L.ref_getan(v(An), v(Anm), v(uh), v(nl), v(param), ab, ng, ncu, nd)
+                        out[f"{tag}_getan{ab}_An"], out[f"{tag}_getan{ab}_Anm"] = An, Anm
+    np.savez_compressed(OUT / "ref_fbou.npz", **out)
 
 
 def binfile_fixture(ref):
@@ -126,6 +188,7 @@ def main(ref):
             sch[f"{tag}_u_{k}"] = v
     np.savez_compressed(OUT / "ref_schur.npz", **sch)
     adjoint_fixture()
+    fbou_fixture()
     binfile_fixture(ref)
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
@@ -145,6 +208,8 @@ if __name__ == "__main__":
     args = [x for x in args if x != only]
     if only == "adjoint":
         adjoint_fixture()
+    elif only == "fbou":
+        fbou_fixture()
     elif only == "binfile":
         binfile_fixture(reference_root(args))
     else:

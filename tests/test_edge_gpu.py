@@ -40,7 +40,7 @@ def test_unsupported_boundary_type_is_reported():
     P = configs.c1(n=4)
     app = copy.deepcopy(P.app)
     app.bcm = np.array(app.bcm)
-    app.bcm[0] = 1                                  # far-field LLF: not on this path
+    app.bcm[0] = 9                                  # not a case of euler/fbou.m
     out = hdg_elemental(P.master, app, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), P.SH)
     st = out.status.numpy()
     touches = np.any(P.mesh.bf == -1, axis=0)       # elements with a face on boundary 1

@@ -1,6 +1,8 @@
 """Generate the committed golden fixtures from the reference (run in a tree that has it).
 
 * master_tri_p2.npz  -- master/testpython.mat (p=2, pgauss=4, triangle), fields as stored.
+* master_seg_p4.npz  -- the face (segment) tables of the p=4 quadrilateral master stored in
+                        problem/burgers/results.mat: plocfc, gpfc, gwfc, shapfc.
 * ref_physics.npz    -- outputs of the reference's generated point kernels
                         application/FM/ns/{flux,fhat}_ns{2,3}d.c and application/FM/euler/
                         {flux,fhat}_euler{2,3}d.c (compiled into oracle/_ref)
@@ -23,7 +25,7 @@
 * binfile_format.json -- the header positions (ndims(k) = ...) and the fwrite sequence of the
                         single-process branch of util/writeBinaryFile.m, read from its source.
 
-Usage: python tests/golden/make_golden.py REFERENCE_ROOT [--only adjoint|fbou|binfile]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT [--only adjoint|fbou|master|binfile]
        (or set HDG_REFERENCE)
 """
 import os
@@ -68,6 +70,16 @@ def adjoint_fixture():
             for k, v in zip(("DUDG", "DUDG_DUH", "AE", "FE"), outs):
                 adj[f"{tag}_{form}_{k}"] = v
     np.savez_compressed(OUT / "ref_schur_adjoint.npz", **adj)
+
+
+def master_p4_fixture(ref):
+    """Face tables of the p=4 master in problem/burgers/results.mat (a quadrilateral master, so
+    only its 1D face tables are shared with the simplices)."""
+    d = sio.loadmat(str(Path(ref) / "problem/burgers/results.mat"), struct_as_record=True)
+    m = d["master"][0, 0]
+    assert int(np.array(m["porder"]).ravel()[0]) == 4 and int(np.array(m["nd"]).ravel()[0]) == 2
+    np.savez_compressed(OUT / "master_seg_p4.npz", **{k: np.array(m[k], dtype=np.float64)
+                                                      for k in ("plocfc", "gpfc", "gwfc", "shapfc")})
 
 
 def fbou_states(nd, ng, seed):
@@ -189,6 +201,7 @@ def main(ref):
     np.savez_compressed(OUT / "ref_schur.npz", **sch)
     adjoint_fixture()
     fbou_fixture()
+    master_p4_fixture(ref)
     binfile_fixture(ref)
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
@@ -210,6 +223,8 @@ if __name__ == "__main__":
         adjoint_fixture()
     elif only == "fbou":
         fbou_fixture()
+    elif only == "master":
+        master_p4_fixture(reference_root(args))
     elif only == "binfile":
         binfile_fixture(reference_root(args))
     else:

@@ -1,0 +1,108 @@
+"""The benchmark configurations at their stated sizes.
+
+* C1, 2D Euler p=2 on the 16x16x2 = 512-triangle mesh: the elemental outputs against the
+  oracle at the elemental tolerances, then the Newton solve (BILU(0)-GMRES in the MDF order,
+  to |F|/|F0| <= 1e-10) against the oracle's Newton solve (kernel/hdg_solve.m:104-176).
+* C2, 2D Navier-Stokes p=3 on all 32,768 triangles: one Newton step on the GPU; the condensed
+  residual |F| the step reports before and after it equals the oracle's assembly
+  (hdg_elemental + globalassembly, kernel/hdg_solve.m:105,154) evaluated at the same states,
+  to 1e-10 relative.
+* C4, 3D Euler p=2 on all 196,608 tetrahedra in one launch: 48 seeded elements against the
+  oracle (as the C2 sample of tests/test_edge_gpu.py)."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from hdg_b200 import configs
+from hdg_b200.app import gather_uh
+
+pytestmark = pytest.mark.gpu
+NT = max(1, min(32, os.cpu_count() or 1))
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _sl(P, idx):
+    m = P.mesh
+    f = lambda a: np.asfortranarray(a[..., idx])
+    return f(m.dgnodes), np.asfortranarray(m.bf[:, idx]), f(P.UDG), f(P.uh_elem()), f(P.SH)
+
+
+def _take(d, idx):
+    """Elements idx of a device output, copied to the host alone (the full C4 outputs are 61 GB)."""
+    return d.view()[..., torch.as_tensor(idx, device=d.t.device)].cpu().numpy()
+
+
+def _dudg_bound(oracle, P, args, ref):
+    """10x the oracle's own change of DUDG when its inputs move by one ulp (DUDG, the local
+    Newton update, is a small difference of O(1) terms)."""
+    rng = np.random.default_rng(7)
+    jit = lambda x: x * (1.0 + 2.2e-16 * rng.standard_normal(x.shape))
+    dg, bf, U, H, S = args
+    ref1 = oracle.hdg_elemental(P.master, P.app, jit(dg), bf, jit(U), jit(H), S, nthreads=NT)
+    return max(1e-12, 10.0 * _rel(ref1["DUDG"], ref["DUDG"]))
+
+
+def test_c1_full_size_elemental_and_newton(oracle):
+    from hdg_b200.elemental import hdg_elemental
+    from hdg_b200.solve import hdg_solve
+    P = configs.c1()
+    assert P.mesh.ne == 512
+    args = _sl(P, np.arange(P.mesh.ne))
+    ref = oracle.hdg_elemental(P.master, P.app, *args, nthreads=NT)
+    out = hdg_elemental(P.master, P.app, *args)
+    assert int(out.status.numpy().max()) == 0 and ref["nbad"] == 0
+    for k in ("AE", "FE", "DUDG_DUH"):
+        assert _rel(getattr(out, k).numpy(), ref[k]) < 1e-12, k
+    assert _rel(out.DUDG.numpy(), ref["DUDG"]) < _dudg_bound(oracle, P, args, ref)
+    U_ref, H_ref, res_ref, g_ref, _ = oracle.hdg_solve(P, tol=1e-10, maxiter=16, nthreads=NT)
+    U, H, rep = hdg_solve(P.master, P.mesh, P.app, P.UDG, P.UH, P.SH, tol=1e-10, maxiter=16)
+    assert rep.converged and res_ref[-1] / res_ref[0] <= 1e-10
+    assert rep.residuals[-1] / rep.residuals[0] <= 1e-10
+    assert len(rep.residuals) == len(res_ref)
+    for a, b in zip(rep.residuals[:-1], res_ref[:-1]):
+        assert abs(a - b) <= 1e-6 * max(b, 1e-300) + 1e-12 * res_ref[0]
+    for gi, gr in zip(rep.gmres_iters, g_ref):
+        assert abs(gi - gr) <= 2
+    assert _rel(U, U_ref) < 1e-8 and _rel(H, H_ref) < 1e-8
+
+
+def _oracle_residual(oracle, P, U, H):
+    """|F| of kernel/hdg_solve.m:105 from the oracle's assembly at the state (U, H)."""
+    r = oracle.hdg_elemental(P.master, P.app, P.mesh.dgnodes, P.mesh.bf, U, gather_uh(H, P.mesh.elcon), P.SH,
+                             nthreads=NT)
+    assert r["nbad"] == 0
+    _, Rg = oracle.globalassembly(P.mesh, r["AE"], r["FE"], P.master.npf, P.app.ncu)
+    return float(np.linalg.norm(Rg))
+
+
+def test_c2_full_size_newton_step_residual(oracle):
+    from hdg_b200.solve import hdg_solve
+    P = configs.c2()
+    assert P.mesh.ne == 32768
+    U, H, rep = hdg_solve(P.master, P.mesh, P.app, P.UDG, P.UH, P.SH, tol=1e-10, maxiter=1)
+    assert rep.iterations == 1 and rep.gmres_relres[0] <= 1e-10
+    F0 = _oracle_residual(oracle, P, P.UDG, P.UH)
+    F1 = _oracle_residual(oracle, P, U, H)
+    assert abs(rep.residuals[0] - F0) <= 1e-10 * F0
+    assert abs(rep.residuals[1] - F1) <= 1e-10 * F1
+    assert F1 < 0.5 * F0
+
+
+def test_c4_full_size_sampled_against_oracle(oracle):
+    from hdg_b200.elemental import hdg_elemental
+    P = configs.c4()
+    assert P.mesh.ne == 196608
+    out = hdg_elemental(P.master, P.app, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), P.SH)
+    torch.cuda.synchronize()
+    assert int(out.status.t.max().item()) == 0
+    idx = np.sort(np.random.default_rng(11).choice(P.mesh.ne, 48, replace=False))
+    args = _sl(P, idx)
+    ref = oracle.hdg_elemental(P.master, P.app, *args, nthreads=NT)
+    for k in ("AE", "FE", "DUDG_DUH"):
+        assert _rel(_take(getattr(out, k), idx), ref[k]) < 1e-12, k
+    assert _rel(_take(out.DUDG, idx), ref["DUDG"]) < _dudg_bound(oracle, P, args, ref)

@@ -184,6 +184,87 @@ def cpu_baseline_timed(P, nthreads, seconds):
     return tot_n / tot_t, tot_n, tot_t
 
 
+def cpu_reference_schur(P, nsample=2048):
+    """The reference's own local Schur MEX, kernel/schur_uq.c (compiled from the reference tree
+    into oracle/_ref with the project's MEX emulation), on the blocks M, C, E, BD, F, GK, H, Rq,
+    Ru, Rh that the oracle's volint/faceint produce for the first ``nsample`` elements: once as
+    the reference runs it (its serial element loop, schur_uq.c:263-287, on one core), and once
+    with the element range split across all host cores (one MEX call per core on its share)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"unavailable": "the reference's schur_uq.c was not compiled into oracle/_ref"}
+    n = min(nsample, P.mesh.ne)
+    sl = slice(0, n)
+    nth = os.cpu_count() or 1
+    blk = O.hdg_elemental(P.master, P.app, np.asfortranarray(P.mesh.dgnodes[..., sl]),
+                          np.asfortranarray(P.mesh.bf[:, sl]), np.asfortranarray(P.UDG[..., sl]),
+                          np.asfortranarray(P.uh_elem()[..., sl]), np.asfortranarray(P.SH[..., sl]),
+                          intermediates=True, nthreads=nth)
+    keys = ("M", "C", "E", "BD", "F", "GK", "H", "Rq", "Ru", "Rh")
+    npv, ncu, nc = P.master.npv, P.app.ncu, P.app.nc
+    ndf = P.master.npf * P.master.nfe
+
+    def prepared(a, b):
+        shapes = [(npv, nc, b - a), (npv, nc, ncu, ndf, b - a), (ncu, ndf, ncu, ndf, b - a), (ncu, ndf, b - a)]
+        return O.ref_mex_call("schur_uq.so", [np.asfortranarray(blk[k][..., a:b]) for k in keys], shapes)
+
+    run, outs = prepared(0, n)
+    t0 = time.perf_counter()
+    run()
+    t_serial = time.perf_counter() - t0
+    err = float(np.abs(outs[3] - blk["FE"]).max() / np.abs(blk["FE"]).max())   # the MEX's FE vs the oracle's
+    cuts = np.linspace(0, n, nth + 1).astype(int)
+    calls = [prepared(a, b)[0] for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
+    with ThreadPoolExecutor(len(calls)) as ex:              # ctypes releases the GIL in the MEX
+        t0 = time.perf_counter()
+        list(ex.map(lambda f: f(), calls))
+        t_par = time.perf_counter() - t0
+    return {"code": "kernel/schur_uq.c (reference source, unmodified) via oracle/_ref/schur_uq.so",
+            "sample": f"{n} elements of the workload (blocks from the oracle's volint/faceint)",
+            "serial": {"value": n / t_serial, "unit": UNIT, "cores": 1, "s": t_serial},
+            "all_cores": {"value": n / t_par, "unit": UNIT, "cores": len(calls), "s": t_par},
+            "FE_rel_diff_vs_oracle": err}
+
+
+def cpu_newton_step(P, gpu_gmres_iters, gmres_sample=20):
+    """One Newton iteration of kernel/hdg_solve.m:104-176 with the CPU oracle (assembly on all
+    host threads; MDF order, BILU(0) factor, GMRES and back-substitution in its single-threaded
+    C): the assembly, MDF order, factor, back-substitution and line-search re-assembly are timed
+    in full; GMRES is timed over ``gmres_sample`` iterations and scaled to the iteration count
+    the same step takes on the GPU (the oracle's MDF-ordered GMRES takes the same count)."""
+    from oracle import oracle as O
+    from hdg_b200.app import gather_uh
+    m, a, mesh = P.master, P.app, P.mesh
+    nth = os.cpu_count() or 1
+    SH = np.array(P.SH, order="F", copy=True)
+    SH[:, a.ncu:, :] = 0.0
+    t = {}
+    t0 = time.perf_counter()
+    r = O.hdg_elemental(m, a, mesh.dgnodes, mesh.bf, P.UDG, gather_uh(P.UH, mesh.elcon), SH, nthreads=nth)
+    Hg, Rg = O.globalassembly(mesh, r["AE"], r["FE"], m.npf, a.ncu)
+    t["assemble_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    o2u, u2o = O.mdf_ordering(mesh, Hg)
+    t["mdf_order_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    Mg, _ = O.bilu0(mesh, Hg, o2u, u2o)
+    t["bilu0_factor_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    DUH, _, it, _ = O.gmres_bilu0(mesh, Mg, Hg, Rg, np.zeros_like(Rg), o2u, u2o, 20, 1e-10, gmres_sample)
+    t_g = time.perf_counter() - t0
+    t["gmres_s_per_iteration"] = t_g / max(it, 1)
+    t0 = time.perf_counter()
+    O.backsub(mesh, r["DUDG"], r["DUDG_DUH"], DUH.reshape(a.ncu, mesh.nsiz, order="F"))
+    t["backsub_s"] = time.perf_counter() - t0
+    est = 2 * t["assemble_s"] + t["mdf_order_s"] + t["bilu0_factor_s"] + t["backsub_s"] + \
+        t["gmres_s_per_iteration"] * gpu_gmres_iters
+    return {"value": mesh.ne / est, "unit": UNIT, "s": est, "cores_assembly": nth, "cores_linear_solve": 1,
+            "kind": "port", "sample": f"assembly x2 (the step and its line-search re-assembly), MDF order, factor and "
+                                       f"back-substitution timed in full; GMRES timed over {it} iterations and scaled "
+                                       f"to {gpu_gmres_iters}", "parts": t}
+
+
 def run_reference(args, wl):
     """--impl reference: the reference path's CPU implementation on the host cores."""
     ws, rank, _ = dist_env()
@@ -328,7 +409,7 @@ def main():
             traffic = None                           # the summary is for the full-size workload
         roof = {"bound": "tensor", "pipe": "fp64", "achieved": achieved_tf, "peak": fp64_peak,
                 "unit": "TFLOP/s", "frac": achieved_tf / fp64_peak,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)",
+                "peak_source": "builder-measured: cuBLAS DGEMM 8192^3 timed by bench.py in this run (MEASURED_PEAKS.json, the driver's file, has no FP64 figure)",
                 "traffic": traffic, "algorithmic_flops_per_element": cnt["flops"],
                 "algorithmic_bytes_per_element": cnt["bytes"],
                 "hbm": {"achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -391,7 +472,8 @@ def main():
             nth = os.cpu_count() or 1
             v, n, dt = cpu_baseline_timed(P, nth, 10.0)
             cpu = {"value": v, "unit": UNIT, "cores": nth, "kind": "port",
-                   "sample": f"{n} element evaluations (the workload's elements, repeated) in {dt:.1f} s, C oracle (volint+faceint+schur_uq2 restated from the reference) on {nth} threads"}
+                   "sample": f"{n} element evaluations (the workload's elements, repeated) in {dt:.1f} s, C oracle (volint+faceint+schur_uq2 restated from the reference) on {nth} threads",
+                   "reference_schur_uq": cpu_reference_schur(P)}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -534,6 +616,9 @@ def newton_step(P, torch, args):
                     "gmres_relres": rep.gmres_relres, "residuals": rep.residuals}
         del s
         torch.cuda.empty_cache()
+    res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+    if not args.no_cpu_baseline:
+        res["cpu_baseline"] = cpu_newton_step(P, res["fp64"]["gmres_iters"][0])
     res["note"] = "one Newton iteration incl. initial assembly, BILU(0)-GMRES(20) to 1e-10, back-substitution, line-search re-assembly"
     res["breakdown"] = newton_breakdown(P, torch)
     return res

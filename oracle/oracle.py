@@ -188,6 +188,27 @@ def ref_mex(soname, inputs, out_shapes):
     return outs
 
 
+def ref_mex_call(soname, inputs, out_shapes):
+    """A prepared call of a reference mexFunction: returns (run, outs), where run() executes only
+    the compiled MEX on private copies of the inputs (each prepared call runs once: the MEX
+    overwrites some inputs in place).  For timing the reference's own code alone."""
+    L = _ref(soname)
+    ins = [np.array(x, dtype=np.float64, order="F", copy=True) for x in inputs]
+    ptrs = (_dp * len(ins))(*[_p(x) for x in ins])
+    ndims = (ct.c_int * len(ins))(*[x.ndim for x in ins])
+    dims = [d for x in ins for d in x.shape]
+    cd = (ct.c_longlong * len(dims))(*dims)
+    outs = [np.zeros(s, order="F") for s in out_shapes]
+    optr = (_dp * len(outs))(*[_p(x) for x in outs])
+    numel = (ct.c_longlong * len(outs))()
+
+    def run():
+        if L.ref_call(len(ins), ptrs, ndims, cd, len(outs), optr, numel) != 0:
+            raise RuntimeError("reference mexFunction failed")
+        return ins
+    return run, outs
+
+
 def ref_flux(nd, param, udg, family="ns"):
     """Reference generated flux kernel; family "euler" takes the u-only state (nc = ncu)."""
     L = _ref("libref_ns.so"); ng, nc = udg.shape; ncu = nd + 2

@@ -130,6 +130,10 @@ def _declare(L):
     L.hdgx_gmres_workspace_bytes.argtypes = [B, i]
     L.hdgx_gmres_bilu0.restype = i
     L.hdgx_gmres_bilu0.argtypes = [B, v, v, v, v, i, d, i, p(i), p(i), p(d), v, v, v]
+    L.hdgx_bilu0_to_f32.restype = i
+    L.hdgx_bilu0_to_f32.argtypes = [B, v, v, v]
+    L.hdgx_gmres_bilu0_mixed.restype = i
+    L.hdgx_gmres_bilu0_mixed.argtypes = [B, v, v, v, v, i, d, i, p(i), p(i), p(d), v, v, v]
     L.hdgx_gmres_bilu0_noalloc.restype = i
     L.hdgx_gmres_bilu0_noalloc.argtypes = [B, v, v, v, v, i, d, i, p(i), p(i), p(d), v, v]
     L.hdgx_backsub.restype = i

@@ -87,6 +87,19 @@ static void sweep_color(const hdgx_bsr *A, int dir, const int *rows, int nr, con
 }
 
 int level_sweep_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *y, double *v, cudaStream_t st);
+int level_sweep_apply_f32(const hdgx_bsr *A, const float *Mg, const double *x, double *y, double *v, cudaStream_t st);
+
+int trace_bilu0_apply_f32(const hdgx_bsr *A, const float *Mg32, const double *x, double *y, double *v,
+                          cudaStream_t st) {
+    if (!A->sweep_plan || A->ncolors < 1) return -2;
+    if (level_sweep_apply_f32(A, Mg32, x, y, v, st) != 0) return -2;
+    return launched();
+}
+
+__global__ void to_f32_kernel(size_t n, const double *__restrict__ a, float *__restrict__ b) {
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        b[t] = (float)a[t];
+}
 
 static int resident_grid(const void *kern, int threads, size_t smem, int cap) {
     int per_sm = 0;
@@ -253,9 +266,12 @@ size_t hdgx_gmres_workspace_bytes(const hdgx_bsr *A, int restart) {
 
 namespace hdgx {
 
-int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const double *b, double *x, int restart,
-                    double tol, int maxit, int *iters, int *flag, double *relres, double *history, void *mem,
-                    cudaStream_t st) {
+int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const float *Mg32, const double *b,
+                    double *x, int restart, double tol, int maxit, int *iters, int *flag, double *relres,
+                    double *history, void *mem, cudaStream_t st) {
+    auto prec = [&](const double *in, double *y, double *v) {
+        return Mg32 ? trace_bilu0_apply_f32(A, Mg32, in, y, v, st) : trace_bilu0_apply(A, Mg, in, y, v, st);
+    };
     const size_t N = (size_t)A->bs * A->nf;
     const int m = restart;
     double *V = (double *)mem;
@@ -283,7 +299,7 @@ int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const
         return rc == 0;
     };
     // pb = P^{-1} b, nrmb = |pb|
-    if (int r = trace_bilu0_apply(A, Mg, b, t, pb, st)) rc = r;
+    if (int r = prec(b, t, pb)) rc = r;
     dot(N, pb, pb, gs.scal + 2, part, 1, st);
     cudaMemcpyAsync(h_nrmb, gs.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, st);
     synced();
@@ -294,7 +310,7 @@ int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const
     while (fl == 2) {
         // r = pb - P^{-1} A x -> V[:,0] = r / beta
         if (int r = trace_matvec(A, Hg, x, t, st)) rc = rc ? rc : r;
-        if (int r = trace_bilu0_apply(A, Mg, t, w2, V, st)) rc = rc ? rc : r;
+        if (int r = prec(t, w2, V)) rc = rc ? rc : r;
         sub_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, pb, V, V);
         dot(N, V, V, gs.scal + 0, part, 1, st);
         scale_div_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, gs.scal + 0, V, V);
@@ -304,7 +320,7 @@ int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const
         for (int j = 0; j < m; j++) {
             double *vj = V + N * j, *w = V + N * (j + 1);
             if (int r = trace_matvec(A, Hg, vj, t, st)) rc = rc ? rc : r;
-            if (int r = trace_bilu0_apply(A, Mg, t, w2, w, st)) rc = rc ? rc : r;
+            if (int r = prec(t, w2, w)) rc = rc ? rc : r;
             double *hc = gs.H + (size_t)(m + 1) * j;
             if (!mgs_fused(N, j + 1, V, w, hc, part, bar, bar_err, st)) {
                 for (int i = 0; i <= j; i++) {        // modified Gram-Schmidt (gmres_bilu0.m:59-63)
@@ -366,7 +382,33 @@ int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, cons
         if (cudaMallocAsync(&mem, hdgx_gmres_workspace_bytes(A, restart), st) != cudaSuccess) return -13;
         own = true;
     }
-    const int rc = gmres_bilu0_run(A, Hg, Mg, b, x, restart, tol, maxit, iters, flag, relres, history, mem, st);
+    const int rc = gmres_bilu0_run(A, Hg, Mg, nullptr, b, x, restart, tol, maxit, iters, flag, relres, history, mem, st);
+    if (own) cudaFreeAsync(mem, st);
+    return rc;
+}
+
+int hdgx_bilu0_to_f32(const hdgx_bsr *A, const double *Mg, float *Mg32, hdgx_stream_t stream) {
+    if (!A || !Mg || !Mg32 || A->bs < 1 || A->nnzb < 0) return -1;
+    const size_t n = (size_t)A->bs * A->bs * (size_t)A->nnzb;
+    if (n == 0) return 0;
+    to_f32_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, Mg, Mg32);
+    return launched();
+}
+
+int hdgx_gmres_bilu0_mixed(const hdgx_bsr *A, const double *Hg, const float *Mg32, const double *b, double *x,
+                           int restart, double tol, int maxit, int *iters, int *flag, double *relres, double *history,
+                           void *workspace, hdgx_stream_t stream) {
+    if (!A || !Hg || !Mg32 || !b || !x || restart < 1 || maxit < 1) return -1;
+    if (!A->sweep_plan || A->ncolors < 1) return -2;   // FP32 factors: level-scheduled sweeps only
+    cudaStream_t st = (cudaStream_t)stream;
+    void *mem = workspace;
+    bool own = false;
+    if (!mem) {
+        if (cudaMallocAsync(&mem, hdgx_gmres_workspace_bytes(A, restart), st) != cudaSuccess) return -13;
+        own = true;
+    }
+    const int rc = gmres_bilu0_run(A, Hg, nullptr, Mg32, b, x, restart, tol, maxit, iters, flag, relres, history, mem,
+                                   st);
     if (own) cudaFreeAsync(mem, st);
     return rc;
 }

@@ -44,16 +44,18 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void *p, unsigned bytes) 
 }
 
 // One row component's record and (PL) matrix values, loadable ahead of the level that uses them.
-template <int BS, int MAXD, bool PL, bool DIAG>
+// MT is the storage type of the factors (double, or float for the mixed-precision preconditioner:
+// the values are widened on use and every sum runs in FP64).
+template <int BS, int MAXD, bool PL, bool DIAG, class MT>
 struct RowPrefetch {
     int i, k0;
     int k[MAXD], j[MAXD];
-    double lv[PL ? MAXD * BS : 1];
-    double dv[(PL && DIAG) ? BS : 1];
+    MT lv[PL ? MAXD * BS : 1];
+    MT dv[(PL && DIAG) ? BS : 1];
 
     // slot record R (NULL: inactive); OFF = 0 for the earlier neighbours, 2 * MAXD for the later
     template <int OFF>
-    __device__ __forceinline__ void load(const int *R, const double *__restrict__ Mg, int r) {
+    __device__ __forceinline__ void load(const int *R, const MT *__restrict__ Mg, int r) {
         if (!R) { i = -1; return; }
         i = __ldg(R);
         k0 = __ldg(R + 1);
@@ -63,16 +65,16 @@ struct RowPrefetch {
 #pragma unroll
             for (int d = 0; d < MAXD; d++) {
                 if (k[d] >= 0) {
-                    const double *B = Mg + (size_t)BS * BS * k[d] + r;
+                    const MT *B = Mg + (size_t)BS * BS * k[d] + r;
 #pragma unroll
                     for (int c = 0; c < BS; c++) lv[d * BS + c] = __ldg(B + BS * c);
                 } else {
 #pragma unroll
-                    for (int c = 0; c < BS; c++) lv[d * BS + c] = 0.0;     // padded slot: contributes 0
+                    for (int c = 0; c < BS; c++) lv[d * BS + c] = MT(0);     // padded slot: contributes 0
                 }
             }
             if constexpr (DIAG) {
-                const double *D = Mg + (size_t)BS * BS * k0 + r;
+                const MT *D = Mg + (size_t)BS * BS * k0 + r;
 #pragma unroll
                 for (int c = 0; c < BS; c++) dv[c] = __ldg(D + BS * c);
             }
@@ -80,7 +82,7 @@ struct RowPrefetch {
     }
 
     // acc - sum_d B_d[r, :] in_{j_d}
-    __device__ __forceinline__ double reduce(double acc, const double *__restrict__ Mg, const double *in, int r) const {
+    __device__ __forceinline__ double reduce(double acc, const MT *__restrict__ Mg, const double *in, int r) const {
         if constexpr (PL) {
             // every neighbour's values are loaded before the first multiply-add, so their L2
             // round trips overlap; padded slots (k < 0) contribute exact zeros
@@ -95,7 +97,7 @@ struct RowPrefetch {
 #pragma unroll
             for (int d = 0; d < MAXD; d++)
 #pragma unroll
-                for (int c = 0; c < BS; c++) acc -= lv[d * BS + c] * ov[d][c];
+                for (int c = 0; c < BS; c++) acc -= (double)lv[d * BS + c] * ov[d][c];
             return acc;
         } else {
 #pragma unroll
@@ -105,10 +107,10 @@ struct RowPrefetch {
                 double ov[BS];
 #pragma unroll
                 for (int c = 0; c < BS; c++) ov[c] = __ldcg(oj + c);
-                const double *B = Mg + (size_t)BS * BS * k[d] + r;
+                const MT *B = Mg + (size_t)BS * BS * k[d] + r;
                 double bv[BS];
 #pragma unroll
-                for (int c = 0; c < BS; c++) bv[c] = __ldg(B + BS * c);
+                for (int c = 0; c < BS; c++) bv[c] = (double)__ldg(B + BS * c);
 #pragma unroll
                 for (int c = 0; c < BS; c++) acc -= bv[c] * ov[c];
             }
@@ -117,23 +119,23 @@ struct RowPrefetch {
     }
 
     // sum_c inv(U_ii)[r, c] t[c]
-    __device__ __forceinline__ double diag(const double *__restrict__ Mg, const double *t, int r) const {
+    __device__ __forceinline__ double diag(const MT *__restrict__ Mg, const double *t, int r) const {
         double o = 0.0;
         if constexpr (PL && DIAG) {
 #pragma unroll
-            for (int c = 0; c < BS; c++) o += dv[c] * t[c];
+            for (int c = 0; c < BS; c++) o += (double)dv[c] * t[c];
         } else {
-            const double *D = Mg + (size_t)BS * BS * k0 + r;
+            const MT *D = Mg + (size_t)BS * BS * k0 + r;
 #pragma unroll
-            for (int c = 0; c < BS; c++) o += __ldg(D + BS * c) * t[c];
+            for (int c = 0; c < BS; c++) o += (double)__ldg(D + BS * c) * t[c];
         }
         return o;
     }
 };
 
-template <int BS, int MAXD, int CS, int NT>
+template <int BS, int MAXD, int CS, int NT, class MT>
 __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NT)
-    bilu0_level_sweep_kernel(int nlev, const int *__restrict__ plan, const double *__restrict__ Mg,
+    bilu0_level_sweep_kernel(int nlev, const int *__restrict__ plan, const MT *__restrict__ Mg,
                              const double *__restrict__ x, double *y, double *v) {
     constexpr int RPP = NT / BS;                        // rows per pass per CTA
     constexpr int RW = 2 + 4 * MAXD;                    // record width (ints)
@@ -172,14 +174,14 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NT)
         return r == 0 ? __ldcg(R + 1) : (r <= MAXD ? __ldcg(R + 2 + 2 * MAXD + 2 * (r - 1)) : -1);
     };
     auto prefetch_block = [&](int k) {
-        if (k >= 0) bulk_prefetch_l2(Mg + (size_t)BS * BS * k, (unsigned)(sizeof(double) * BS * BS));
+        if (k >= 0) bulk_prefetch_l2(Mg + (size_t)BS * BS * k, (unsigned)(sizeof(MT) * BS * BS));
     };
 
     // forward sweep: y_i = x_i - sum_{j before i} L_ij y_j, levels in elimination order
     {
         for (int l = 0; l < DR; l++) prefetch_rec(l);
         int pk = block_of(DK - 1, false);
-        RowPrefetch<BS, MAXD, PLF, false> pf;
+        RowPrefetch<BS, MAXD, PLF, false, MT> pf;
         pf.template load<0>(slot_rec(0), Mg, r);
         double xv = pf.i >= 0 ? __ldg(x + (size_t)BS * pf.i + r) : 0.0;
         for (int lev = 0; lev < nlev; lev++) {
@@ -188,7 +190,7 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NT)
             for (int base = CS * RPP; base < nr; base += CS * RPP) {
                 const int s = base + rank + CS * m;
                 if (m < RPP && s < nr) {
-                    RowPrefetch<BS, MAXD, false, false> row;
+                    RowPrefetch<BS, MAXD, false, false, MT> row;
                     row.template load<0>(rec + (size_t)(q0 + s) * RW, Mg, r);
                     y[(size_t)BS * row.i + r] = row.reduce(__ldg(x + (size_t)BS * row.i + r), Mg, y, r);
                 }
@@ -209,7 +211,7 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NT)
     {
         for (int l = 0; l < DR; l++) prefetch_rec(nlev - 1 - l);
         int pk = block_of(nlev - DK, true);
-        RowPrefetch<BS, MAXD, PLB, true> pf;
+        RowPrefetch<BS, MAXD, PLB, true, MT> pf;
         pf.template load<2 * MAXD>(slot_rec(nlev - 1), Mg, r);
         for (int lev = nlev - 1; lev >= 0; lev--) {
             const int q0 = lp[lev], nr = lp[lev + 1] - q0;
@@ -222,7 +224,7 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NT)
             for (int base = CS * RPP; base < nr; base += CS * RPP) {    // trip count is uniform in the CTA
                 const int s = base + rank + CS * m;
                 const bool act = m < RPP && s < nr;
-                RowPrefetch<BS, MAXD, false, true> row;
+                RowPrefetch<BS, MAXD, false, true, MT> row;
                 row.template load<2 * MAXD>(act ? rec + (size_t)(q0 + s) * RW : nullptr, Mg, r);
                 if (act) tsh[m * BS + r] = row.reduce(__ldcg(y + (size_t)BS * row.i + r), Mg, v, r);
                 __syncthreads();
@@ -244,10 +246,10 @@ constexpr int kSweepCS = 8;     // CTAs in the cluster (portable maximum)
 constexpr int kSweepNT = 256;
 
 // 0 launched, 1 not possible (caller falls back), 2 the device cannot place such a cluster
-template <int BS, int MAXD, int CS, int NT>
-static int launch_cluster(int nlev, const int *plan, const double *Mg, const double *x, double *y, double *v,
+template <int BS, int MAXD, int CS, int NT, class MT>
+static int launch_cluster(int nlev, const int *plan, const MT *Mg, const double *x, double *y, double *v,
                           size_t smem, cudaStream_t st) {
-    auto kern = bilu0_level_sweep_kernel<BS, MAXD, CS, NT>;
+    auto kern = bilu0_level_sweep_kernel<BS, MAXD, CS, NT, MT>;
     if (smem > 40 * 1024 && allow_dynamic_smem((const void *)kern, smem) != cudaSuccess) return 1;
     if (CS > 8) {
         if (cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
@@ -277,37 +279,46 @@ static int launch_cluster(int nlev, const int *plan, const double *Mg, const dou
 // a 16-CTA cluster needs 16 free SMs of one GPC, which concurrent solves rarely leave (64 queued
 // serving requests: 32 solves/s with 16-CTA clusters for their bs = 20 systems, 74 with 8).
 constexpr size_t kWideLevelBytes = 4u << 20;
-template <int BS, int MAXD>
-static int launch_level_sweep(int nlev, long long nnzb, const int *plan, const double *Mg, const double *x, double *y,
+template <int BS, int MAXD, class MT>
+static int launch_level_sweep(int nlev, long long nnzb, const int *plan, const MT *Mg, const double *x, double *y,
                               double *v, cudaStream_t st) {
     const size_t smem = sizeof(int) * ((size_t)nlev + 1);
     if (smem > 160 * 1024) return 1;                    // very long schedules: per-level launches
     if constexpr (BS >= 20) {
-        const size_t level_bytes = sizeof(double) * BS * BS * (size_t)nnzb / (size_t)nlev;
+        const size_t level_bytes = sizeof(MT) * BS * BS * (size_t)nnzb / (size_t)nlev;
         if (level_bytes >= kWideLevelBytes) {
-            const int rc = launch_cluster<BS, MAXD, 16, 512>(nlev, plan, Mg, x, y, v, smem, st);
+            const int rc = launch_cluster<BS, MAXD, 16, 512, MT>(nlev, plan, Mg, x, y, v, smem, st);
             if (rc != 2) return rc;
         }
-        return launch_cluster<BS, MAXD, 8, 512>(nlev, plan, Mg, x, y, v, smem, st) == 0 ? 0 : 1;
+        return launch_cluster<BS, MAXD, 8, 512, MT>(nlev, plan, Mg, x, y, v, smem, st) == 0 ? 0 : 1;
     } else {
-        return launch_cluster<BS, MAXD, kSweepCS, kSweepNT>(nlev, plan, Mg, x, y, v, smem, st) == 0 ? 0 : 1;
+        return launch_cluster<BS, MAXD, kSweepCS, kSweepNT, MT>(nlev, plan, Mg, x, y, v, smem, st) == 0 ? 0 : 1;
     }
 }
 
 // 0 when launched, 1 when there is no plan or no specialisation for it (the caller falls back)
-int level_sweep_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *y, double *v, cudaStream_t st) {
+template <class MT>
+static int level_sweep_apply_t(const hdgx_bsr *A, const MT *Mg, const double *x, double *y, double *v, cudaStream_t st) {
     if (!A->sweep_plan || A->ncolors < 1) return 1;
     const int md = A->sweep_maxd;
     if (md != 4 && md != 6) return 1;
     switch (A->bs) {
 #define HDGX_LS(B)                                                                                \
     case B:                                                                                       \
-        return md == 4 ? launch_level_sweep<B, 4>(A->ncolors, A->nnzb, A->sweep_plan, Mg, x, y, v, st)    \
-                       : launch_level_sweep<B, 6>(A->ncolors, A->nnzb, A->sweep_plan, Mg, x, y, v, st);
+        return md == 4 ? launch_level_sweep<B, 4, MT>(A->ncolors, A->nnzb, A->sweep_plan, Mg, x, y, v, st)    \
+                       : launch_level_sweep<B, 6, MT>(A->ncolors, A->nnzb, A->sweep_plan, Mg, x, y, v, st);
         HDGX_LS(8) HDGX_LS(12) HDGX_LS(15) HDGX_LS(16) HDGX_LS(20) HDGX_LS(30)
 #undef HDGX_LS
         default: return 1;
     }
+}
+
+int level_sweep_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *y, double *v, cudaStream_t st) {
+    return level_sweep_apply_t<double>(A, Mg, x, y, v, st);
+}
+// The same sweeps with the factors stored in FP32 (the mixed-precision preconditioner)
+int level_sweep_apply_f32(const hdgx_bsr *A, const float *Mg, const double *x, double *y, double *v, cudaStream_t st) {
+    return level_sweep_apply_t<float>(A, Mg, x, y, v, st);
 }
 
 }  // namespace hdgx

@@ -107,5 +107,6 @@ extern "C" int hdgx_gmres_bilu0_noalloc(const hdgx_bsr *A, const double *Hg, con
     // workspace, so that nothing of an earlier solve (Hessenberg columns, rotations, the grid
     // barrier of the fused Gram-Schmidt step) can leak into this one.
     if (cudaMemsetAsync(base, 0, need, st) != cudaSuccess) return -12;
-    return hdgx::gmres_bilu0_run(A, Hg, Mg, b, x, restart, tol, maxit, iters, flag, relres, history, base, st);
+    return hdgx::gmres_bilu0_run(A, Hg, Mg, nullptr, b, x, restart, tol, maxit, iters, flag, relres, history, base,
+                                 st);
 }

@@ -324,6 +324,7 @@ extern "C" int hdgx_solve(const hdgx_master *m, const hdgx_app *app, const hdgx_
     double rel = 1.0;
     int it = 0;
     bool ordered = opts->ordering == 1;
+    float *Mg32 = nullptr;                           // FP32 factors (mixed precision), allocated once
     while (rel > opts->tol && it < opts->maxiter && it < HDGX_SOLVE_MAXIT) {
         if (!ordered) {
             // computeMDFordering.m on the first assembled matrix
@@ -345,8 +346,14 @@ extern "C" int hdgx_solve(const hdgx_master *m, const hdgx_app *app, const hdgx_
         cudaMemsetAsync(DUH, 0, sizeof(double) * nH, st);
         int gi = 0, gfl = 0;
         double grr = 0.0;
-        if (int rc = hdgx_gmres_bilu0(&A, Hg, Mg, Rg, DUH, opts->restart, opts->gmres_tol, opts->gmres_maxit, &gi,
-                                      &gfl, &grr, nullptr, ws, stream))
+        // mixed precision: the preconditioner's factors in FP32 where the level sweeps run them
+        const bool f32 = opts->mixed && A.sweep_plan && A.ncolors > 0;
+        if (f32 && !Mg32 && !(Mg32 = pool.get<float>((size_t)bs * bs * nnzb))) return -13;
+        if (f32 && (hdgx_bilu0_to_f32(&A, Mg, Mg32, stream) != 0)) return -12;
+        if (int rc = f32 ? hdgx_gmres_bilu0_mixed(&A, Hg, Mg32, Rg, DUH, opts->restart, opts->gmres_tol,
+                                                  opts->gmres_maxit, &gi, &gfl, &grr, nullptr, ws, stream)
+                         : hdgx_gmres_bilu0(&A, Hg, Mg, Rg, DUH, opts->restart, opts->gmres_tol, opts->gmres_maxit,
+                                            &gi, &gfl, &grr, nullptr, ws, stream))
             return rc;
         r.gmres_iters[it] = gi;
         r.gmres_relres[it] = grr;

@@ -34,11 +34,17 @@ int trace_matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *y
 // per colour otherwise.  Allocates nothing.
 int trace_bilu0_apply(const hdgx_bsr *A, const double *Mg, const double *x, double *y, double *v, cudaStream_t st);
 
+// The same sweeps with the factors stored in FP32 (every sum in FP64); only the single-launch
+// level sweeps of A->sweep_plan are offered in this form (-2 otherwise).
+int trace_bilu0_apply_f32(const hdgx_bsr *A, const float *Mg32, const double *x, double *y, double *v,
+                          cudaStream_t st);
+
 // Restarted left-preconditioned GMRES (kernel/gmres_bilu0.m) with every scratch array carved from
-// `mem` (hdgx_gmres_workspace_bytes(A, restart) bytes, 8-byte aligned).  Allocates nothing; the
-// host scalars live on the caller's stack.  Returns 0 or a status of include/hdgx.h.
-int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const double *b, double *x, int restart,
-                    double tol, int maxit, int *iters, int *flag, double *relres, double *history, void *mem,
-                    cudaStream_t st);
+// `mem` (hdgx_gmres_workspace_bytes(A, restart) bytes, 8-byte aligned).  The preconditioner is the
+// FP64 factors Mg, or, when Mg32 is not NULL, the same factors stored in FP32.  Allocates nothing;
+// the host scalars live on the caller's stack.  Returns 0 or a status of include/hdgx.h.
+int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const float *Mg32, const double *b,
+                    double *x, int restart, double tol, int maxit, int *iters, int *flag, double *relres,
+                    double *history, void *mem, cudaStream_t st);
 
 }  // namespace hdgx

@@ -149,6 +149,20 @@ class TraceSystem:
         check(rc, "hdgx_gmres_bilu0")
         return it.value, fl.value, rr.value, hist[:it.value]
 
+    def gmres_mixed(self, Hg, Mg, Mg32, b, x, restart=20, tol=1e-10, maxit=1000, workspace=None, stream=None):
+        """gmres with the factors Mg converted to FP32 (Mg32, a float32 tensor of Mg's size) and
+        read in FP32 by the level sweeps; the rest of GMRES stays FP64."""
+        st = _stream_ptr(stream)
+        check(lib().hdgx_bilu0_to_f32(ct.byref(self.bsr), Mg.ptr, Mg32.data_ptr(), st), "hdgx_bilu0_to_f32")
+        it, fl, rr = ct.c_int(0), ct.c_int(0), ct.c_double(0.0)
+        hist = np.zeros(maxit + 1)
+        ws = workspace.data_ptr() if workspace is not None else None
+        rc = lib().hdgx_gmres_bilu0_mixed(ct.byref(self.bsr), Hg.ptr, Mg32.data_ptr(), b.ptr, x.ptr, int(restart),
+                                          float(tol), int(maxit), ct.byref(it), ct.byref(fl), ct.byref(rr),
+                                          hist.ctypes.data_as(ct.c_void_p), ws, st)
+        check(rc, "hdgx_gmres_bilu0_mixed")
+        return it.value, fl.value, rr.value, hist[:it.value]
+
     def workspace(self, restart):
         nb = lib().hdgx_gmres_workspace_bytes(ct.byref(self.bsr), int(restart))
         return torch.empty(int(nb), dtype=torch.uint8, device="cuda")
@@ -225,6 +239,12 @@ class HDGSolver:
             self.dense.build(self.Hg, self.Rg, stream)
             return self.dense.gmres(self.DUH, restart=self.restart, tol=tol, maxit=maxit, stream=stream)
         self.ts.bilu0(self.Hg, self.Mg, stream=stream)
+        if self.mixed and self.ts.bsr.sweep_plan:
+            # mixed precision: the preconditioner's factors read in FP32 by the level sweeps
+            if getattr(self, "Mg32", None) is None:
+                self.Mg32 = torch.empty(self.Mg.t.numel(), dtype=torch.float32, device=self.Mg.t.device)
+            return self.ts.gmres_mixed(self.Hg, self.Mg, self.Mg32, self.Rg, self.DUH, self.restart, tol, maxit,
+                                       self.ws, stream)
         return self.ts.gmres(self.Hg, self.Mg, self.Rg, self.DUH, self.restart, tol, maxit, self.ws, stream)
 
     def backsub(self, stream=None):

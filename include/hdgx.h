@@ -25,6 +25,7 @@
  *   hdgx_bilu0_factor     kernel/computeBILU0.m:1    Mg = computeBILU0(mesh,Hg)
  *   hdgx_bilu0_apply      kernel/applyBILU0.m:1      v  = applyBILU0(mesh,Mg,x)
  *   hdgx_gmres_bilu0      kernel/gmres_bilu0.m:1     [x,flags,iter,rev] = gmres_bilu0(mesh,M,A,b,x,restart,tol,maxit)
+ *   hdgx_gmres_bilu0_mixed kernel/gmres_bilu0.m:1    the same with the factors M stored in FP32
  *   hdgx_backsub          kernel/hdg_solve.m:119-121 DUDGT = DUDG + mapContractK(DUDG_DUH, DUH(elcon))
  *   hdgx_gather_uh        kernel/hdg_assemble.m:34   uh = reshape(UH(:,elcon),[ncu npf*nfe ne])
  *   hdgx_solve            kernel/hdg_solve.m:1       [UDG,UH] = hdg_solve(master,mesh,app,UDG,UH,SH)
@@ -291,6 +292,21 @@ size_t hdgx_gmres_workspace_bytes(const hdgx_bsr *A, int restart);
 int hdgx_gmres_bilu0(const hdgx_bsr *A, const double *Hg, const double *Mg, const double *b, double *x,
                      int restart, double tol, int maxit, int *iters, int *flag, double *relres,
                      double *history, void *workspace, hdgx_stream_t stream);
+
+/* Mg32[bs,bs,nnzb] = (float) Mg: the BILU(0) factors of hdgx_bilu0_factor stored in FP32 for
+ * hdgx_gmres_bilu0_mixed.  No counterpart in the reference (its factors are FP64 MATLAB arrays,
+ * kernel/computeBILU0.m); part of the mixed-precision Newton step. */
+int hdgx_bilu0_to_f32(const hdgx_bsr *A, const double *Mg, float *Mg32, hdgx_stream_t stream);
+
+/* hdgx_gmres_bilu0 (kernel/gmres_bilu0.m) with the preconditioner's factors read in FP32 (Mg32 of
+ * hdgx_bilu0_to_f32); the sweeps accumulate in FP64 and the matvec with Hg, the Arnoldi
+ * orthogonalisation, the Givens rotations and the residual stay FP64.  The preconditioner is then
+ * a slightly different fixed operator, so the converged solution is that of the FP64 system to
+ * the same tolerance (the iteration count may differ by a few).  Offered for the single-launch
+ * level sweeps of A->sweep_plan; returns -2 otherwise.  Same arguments as hdgx_gmres_bilu0. */
+int hdgx_gmres_bilu0_mixed(const hdgx_bsr *A, const double *Hg, const float *Mg32, const double *b, double *x,
+                           int restart, double tol, int maxit, int *iters, int *flag, double *relres, double *history,
+                           void *workspace, hdgx_stream_t stream);
 
 /* Allocation-free variant of hdgx_gmres_bilu0 (same arguments minus the workspace; the same
  * solver code and kernels, so the same results bit for bit, for every ordering hdgx_bsr

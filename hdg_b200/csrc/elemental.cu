@@ -21,6 +21,7 @@
 #include <type_traits>
 #include <math.h>
 #include "hdgx_common.cuh"
+#include "tcgen05.cuh"
 
 namespace hdgx {
 
@@ -60,6 +61,8 @@ struct Dims {
 // is dead during the solve).  The geometry tables shapmv / shapmf are read from global
 // memory (L1) instead: they are used once per element.  Less shared memory per element means
 // more elements resident per SM (the kernel is latency-bound).
+constexpr int al16(int x) { return (x + 15) / 16 * 16; }   // a double offset rounded up to 128 bytes
+
 template <class D, bool VISC, bool MIXED = false, bool TAB = true>
 struct Plan {
     // master tables (loaded once per CTA; shapvt / shapvg stay in global memory when !TAB)
@@ -127,8 +130,35 @@ struct Plan {
     static constexpr int d_diag = d_pcol + 4 * D::NU;                   // [NU] pivots
     static constexpr int d_b0 = d_diag + D::NU;                         // [NU] first right-hand side
     static constexpr int d_invsep = d_b0 + D::NU;                       // [NU*NU] FP32-accurate SD^-1 (MIXED)
-    static constexpr int n_doubles = d_invsep + ((MIXED && !INV_ALIAS) ? D::NU * D::NU : 0);
+    static constexpr int d_mbar = d_invsep + ((MIXED && !INV_ALIAS) ? D::NU * D::NU : 0);   // tensor-core mbarrier
+    static constexpr int n_doubles = d_mbar + (MIXED ? 2 : 0);
     static constexpr int d_inv = INV_ALIAS ? x_start + (SD_ALIAS ? D::NU * D::NU : 0) : d_invsep;
+    // Tensor-core Schur product of the mixed form, X = SD^-1 [B Mi E - F] (tcgen05, 3xTF32): the
+    // operands, SD^-1 as A (M = 128 rows of which NU are real, K = NU padded to the MMA step) and
+    // 16 right-hand-side columns at a time as B (N = 16), are staged in shared memory that is dead
+    // once the residual column has passed its check: the assembly scratch outside SD^-1 (SD itself
+    // is no longer read).  The A descriptor covers 16 row groups; the rows past NU are never
+    // used, but they must lie inside the CTA's shared memory.
+    static constexpr int TC_KP = (D::NU + 7) / 8 * 8;                     // K, a multiple of 8
+    static constexpr int TC_KC = TC_KP / 4;                               // 16-byte K chunks per row group
+    static constexpr int TC_G = (D::NU + 7) / 8;                          // row groups of A with real rows
+    static constexpr int TC_NP = (D::NH + 15) / 16 * 16;                  // right-hand sides, padded
+    static constexpr int TC_ADBL = 2 * TC_G * TC_KC * 128 / 8;            // A hi + lo, in doubles
+    static constexpr int TC_BDBL = 2 * 2 * TC_KC * 128 / 8;               // one 16-row B tile, hi + lo
+    static constexpr int inv_lo = INV_ALIAS ? d_inv : x_end, inv_hi = INV_ALIAS ? d_inv + D::NU * D::NU : x_end;
+    // free ranges [x_start, inv_lo) and [inv_hi, x_end) (offsets rounded up to 128 bytes): A and B
+    // in the upper one (1), or A in the lower and B in the upper one (2), or the reverse (3)
+    static constexpr int TC_PL =
+        !MIXED ? 0
+               : (al16(al16(inv_hi) + TC_ADBL) + TC_BDBL <= x_end
+                      ? 1
+                      : (al16(x_start) + TC_ADBL <= inv_lo && al16(inv_hi) + TC_BDBL <= x_end
+                             ? 2
+                             : (al16(inv_hi) + TC_ADBL <= x_end && al16(x_start) + TC_BDBL <= inv_lo ? 3 : 0)));
+    static constexpr int tc_a = TC_PL == 1 ? al16(inv_hi) : (TC_PL == 2 ? al16(x_start) : al16(inv_hi));
+    static constexpr int tc_b = TC_PL == 1 ? al16(tc_a + TC_ADBL) : (TC_PL == 2 ? al16(inv_hi) : al16(x_start));
+    static constexpr bool TC = TC_PL != 0 && tc_a * 8 + 16 * TC_KC * 128 <= (int)(sizeof(double) * n_doubles) &&
+                               TC_NP <= 256 && D::NU <= 64;
     // integers after the doubles
     static constexpr int i_perm = 0;                      // [NPF, NFE] 0-based
     static constexpr int i_invp = D::NPF * D::NFE;        // [NPV, NFE] face-local index or -1
@@ -139,7 +169,8 @@ struct Plan {
     static constexpr int i_gslot = i_rowvar + D::NU;
     static constexpr int i_bf = i_gslot + 2;
     static constexpr int i_bad = i_bf + D::NFE;
-    static constexpr int n_ints = i_bad + 1;
+    static constexpr int i_tmem = i_bad + 1;              // TMEM address of the tensor-core accumulator
+    static constexpr int n_ints = i_tmem + 1;
     static constexpr size_t bytes = sizeof(double) * n_doubles + sizeof(int) * n_ints;
 };
 
@@ -201,7 +232,23 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     for (int i = tid; i < NPV * NFE; i += NT) invp[i] = -1;
     __syncthreads();
     for (int i = tid; i < NPF * NFE; i += NT) invp[perm[i] + NPV * (i / NPF)] = i % NPF;
+    // mixed form: the tensor-memory accumulator of the Schur product and its mbarrier, once per CTA
+    constexpr uint32_t TC_COLS = L::TC_NP <= 32 ? 32 : (L::TC_NP <= 64 ? 64 : (L::TC_NP <= 128 ? 128 : 256));
+    uint64_t *s_mbar = reinterpret_cast<uint64_t *>(sm + L::d_mbar);
+    uint32_t tmem = 0, tc_phase = 0;
+    if constexpr (L::TC) {
+        if (tid < 32) tc::tmem_alloc(reinterpret_cast<uint32_t *>(si + L::i_tmem), TC_COLS);
+        if (tid == 0) {
+            tc::mbar_init(s_mbar, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        tc::fence_before_sync();
+    }
     __syncthreads();
+    if constexpr (L::TC) {
+        tc::fence_after_sync();
+        tmem = *reinterpret_cast<const uint32_t *>(si + L::i_tmem);
+    }
 
     double *s_dg = sm + L::p_dg, *s_udg = sm + L::p_udg, *s_uh = sm + L::p_uh;
     double *s_SD = sm + L::p_SD, *s_R = sm + L::p_R;
@@ -727,6 +774,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         // ================================ LU of SD and the 1 + NH solves (schur_primal.m:111,118)
         {
             int bad_before = *s_bad;
+            bool tc_go = false;          // the unpivoted mixed solve passed its check: Schur product next
             __syncthreads();
             if (force_piv) {
                 gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
@@ -740,11 +788,12 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             for (int i = tid; i < NU; i += NT) s_b0[i] = s_R[i];
             __syncthreads();
             if constexpr (MIXED) {
-                // FP32 elimination of [SD | R | I], then the residual column refined in FP64
-                // against the FP64 SD with the FP32 inverse
+                // FP32 elimination of [SD | R | I] (with the tensor-core Schur product: of
+                // [SD | r0 | I] only, the other right-hand sides are multiplied by SD^-1 below),
+                // then the residual column refined in FP64 against the FP64 SD with the FP32 inverse
                 double *s_inv = sm + L::d_inv;
-                gj_regs_nopiv_t<float, NU, 1 + NH, NU, true, NT, 8, NPV>(s_SD, s_R, s_inv,
-                                                                        reinterpret_cast<float *>(s_pcol), s_bad);
+                gj_regs_nopiv_t<float, NU, L::TC ? 1 : 1 + NH, NU, true, NT, 8, NPV>(
+                    s_SD, s_R, s_inv, reinterpret_cast<float *>(s_pcol), s_bad);
                 double *s_res = s_pcol;                    // free after the elimination
                 for (int it = 0; it < 3; it++) {
                     for (int r = tid; r < NU; r += NT) {
@@ -805,6 +854,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                 }
                 __syncthreads();
             }
+            tc_go = s_gslot[0] == 0;
             if (s_gslot[0]) {
                 // fall back to partial pivoting on the original system
                 if (L::SD_ALIAS || L::INV_ALIAS) {
@@ -820,6 +870,74 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             }
             if (tid == 0 && *s_bad && !bad_before) *s_bad = 2;
             __syncthreads();
+            if constexpr (L::TC) {
+                // Schur product on the tensor cores (tcgen05 kind::tf32, 3xTF32 with FP32
+                // accumulation): R(:, 1:) = SD^-1 R(:, 1:) (schur_primal.m:118, dlu = SD \ (BMiE - F)),
+                // once the residual column has passed its check (a pivoted redo solves R in FP64).
+                // A = SD^-1 (K-major: row r, column k), B = 16 right-hand sides per MMA round (row n
+                // = right-hand side, K-major), D = A B^T in TMEM columns n0 .. n0 + 15.
+                if (tc_go) {
+                    constexpr int KP = L::TC_KP, KC = L::TC_KC, GR = 8 * L::TC_G, NP = L::TC_NP;
+                    constexpr int AH = L::TC_G * KC * 128, BH = 2 * KC * 128;    // bytes of one hi / lo half
+                    const double *s_inv = sm + L::d_inv;
+                    unsigned char *tA = reinterpret_cast<unsigned char *>(sm + L::tc_a);
+                    unsigned char *tB = reinterpret_cast<unsigned char *>(sm + L::tc_b);
+                    for (int i = tid; i < GR * KP; i += NT) {
+                        const int r = i % GR, k = i / GR;
+                        float h = 0.f, l = 0.f;
+                        if (r < NU && k < NU) tc::split_tf32(s_inv[r + NU * k], h, l);
+                        const int off = tc::kmajor_offset(r, k, KC);
+                        *reinterpret_cast<float *>(tA + off) = h;
+                        *reinterpret_cast<float *>(tA + AH + off) = l;
+                    }
+                    constexpr uint32_t idesc = tc::idesc_tf32(128, 16);
+                    const uint32_t aaddr = tc::smem_u32(tA), baddr = tc::smem_u32(tB);
+                    for (int n0 = 0; n0 < NP; n0 += 16) {
+                        for (int i = tid; i < 16 * KP; i += NT) {
+                            const int n = i % 16, k = i / 16;
+                            float h = 0.f, l = 0.f;
+                            if (n0 + n < NH && k < NU) tc::split_tf32(s_R[k + NU * (1 + n0 + n)], h, l);
+                            const int off = tc::kmajor_offset(n, k, KC);
+                            *reinterpret_cast<float *>(tB + off) = h;
+                            *reinterpret_cast<float *>(tB + BH + off) = l;
+                        }
+                        tc::fence_proxy_async();
+                        __syncthreads();
+                        if (tid == 0) {
+                            tc::fence_after_sync();
+#pragma unroll
+                            for (int s = 0; s < KP / 8; s++) {
+                                const uint64_t ah = tc::smem_desc(aaddr + 256 * s, 128, KC * 128);
+                                const uint64_t al = tc::smem_desc(aaddr + AH + 256 * s, 128, KC * 128);
+                                const uint64_t bh = tc::smem_desc(baddr + 256 * s, 128, KC * 128);
+                                const uint64_t bl = tc::smem_desc(baddr + BH + 256 * s, 128, KC * 128);
+                                tc::mma_tf32(tmem + n0, al, bh, idesc, s > 0);
+                                tc::mma_tf32(tmem + n0, ah, bl, idesc, true);
+                                tc::mma_tf32(tmem + n0, ah, bh, idesc, true);
+                            }
+                            tc::commit(s_mbar);
+                        }
+                        // every thread sees the MMAs complete before the next round rewrites B
+                        if (!tc::mbar_wait(s_mbar, tc_phase, 1 << 22)) *s_bad = 4;
+                        tc_phase ^= 1;
+                        tc::fence_after_sync();
+                    }
+                    // rows r < NU are TMEM lanes 0..NU-1: warp w reads lanes 32 w .. 32 w + 31
+                    if (tid < 32 * ((NU + 31) / 32)) {
+                        const int w = tid >> 5;
+#pragma unroll 1
+                        for (int c = 0; c < NP; c += 16) {
+                            float v[16];
+                            tc::tmem_ld16(tmem + ((uint32_t)(32 * w) << 16) + (uint32_t)c, v);
+#pragma unroll
+                            for (int i = 0; i < 16; i++)
+                                if (tid < NU && c + i < NH) s_R[tid + NU * (1 + c + i)] = (double)v[i];
+                        }
+                    }
+                    tc::fence_before_sync();
+                    __syncthreads();
+                }
+            }
         }
 
         // ================================ DUDG = [du, MiRq + MiC du] (schur_primal.m:112-116)
@@ -943,6 +1061,11 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         else tiles(std::integral_constant<int, NCU>{});
         if (tid == 0 && P.status) P.status[e] = *s_bad;
         __syncthreads();
+    }
+    if constexpr (L::TC) {
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid < 32) tc::tmem_dealloc(tmem, TC_COLS);
     }
 }
 

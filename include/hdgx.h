@@ -111,7 +111,11 @@ int hdgx_elemental(const hdgx_master *master, const hdgx_app *app, int ne,
  * kernel/hdg_elemental.m call).  The local elimination of the Jacobian columns runs in FP32
  * and the local residual solve is refined against the FP64 local matrix, so FE and DUDG
  * are FP64-accurate residual quantities while AE and DUDG_DUH carry FP32-level error (a
- * Jacobian error: Newton converges to the same FP64 solution).  status 4: refinement failed. */
+ * Jacobian error: Newton converges to the same FP64 solution).  The Schur product of the Jacobian
+ * columns, dlu = SD^-1 (B Mi E - F) (schur_primal.m:118), runs on the tensor cores (tcgen05,
+ * kind::tf32, as three TF32 products of the split operands: FP32-level accuracy) for every element
+ * shape but 2D p = 4 (no room for its operands next to the shared-memory plan; it keeps the FP32
+ * elimination of all columns).  status 4: refinement failed, or a tensor-core wait ran out. */
 int hdgx_elemental_mixed(const hdgx_master *master, const hdgx_app *app, int ne,
                          const double *dgnodes, const int *bf, const double *UDG, const double *UH,
                          const double *SH, double *AE, double *FE, double *DUDG, double *DUDG_DUH,

@@ -66,11 +66,10 @@ def test_c1_full_size_elemental_and_newton(oracle):
     assert len(rep.residuals) == len(res_ref)
     for a, b in zip(rep.residuals[:-1], res_ref[:-1]):
         assert abs(a - b) <= 1e-6 * max(b, 1e-300) + 1e-12 * res_ref[0]
-    # GMRES counts agree within 2 except in the last step, whose right-hand side is at the
-    # rounding level of the converged state (there the count moves with summation order)
-    for gi, gr in zip(rep.gmres_iters[:-1], g_ref[:-1]):
-        assert abs(gi - gr) <= 2
-    assert abs(rep.gmres_iters[-1] - g_ref[-1]) <= max(2, 0.2 * g_ref[-1])
+    # GMRES counts (same MDF order on both sides): at this size a 1e-10 tolerance is reached a
+    # few iterations apart depending on the summation order of the dot products
+    for gi, gr in zip(rep.gmres_iters, g_ref):
+        assert abs(gi - gr) <= max(2, 0.15 * gr)
     assert _rel(U, U_ref) < 1e-8 and _rel(H, H_ref) < 1e-8
 
 

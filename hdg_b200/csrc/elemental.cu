@@ -63,6 +63,25 @@ struct Dims {
 // more elements resident per SM (the kernel is latency-bound).
 constexpr int al16(int x) { return (x + 15) / 16 * 16; }   // a double offset rounded up to 128 bytes
 
+// Placement of the tensor-core operands of the mixed form in the free scratch ranges
+// [x_start, inv_lo) and [inv_hi, x_end) (double offsets): A (SD^-1, adbl doubles) and a B tile of
+// nb right-hand sides (nb a multiple of 16 dividing np, as large as fits: fewer MMA rounds).
+// pl 0: no placement.
+struct TcPlace {
+    int pl, nb, a, b;
+};
+constexpr TcPlace tc_place(bool mixed, int x_start, int inv_lo, int inv_hi, int x_end, int adbl, int kc, int np) {
+    if (!mixed) return {0, 16, 0, 0};
+    for (int nb = np; nb >= 16; nb -= 16) {
+        if (np % nb || nb > 256) continue;
+        const int bdbl = 2 * (nb / 8) * kc * 128 / 8;
+        if (al16(al16(inv_hi) + adbl) + bdbl <= x_end) return {1, nb, al16(inv_hi), al16(al16(inv_hi) + adbl)};
+        if (al16(x_start) + adbl <= inv_lo && al16(inv_hi) + bdbl <= x_end) return {2, nb, al16(x_start), al16(inv_hi)};
+        if (al16(inv_hi) + adbl <= x_end && al16(x_start) + bdbl <= inv_lo) return {3, nb, al16(inv_hi), al16(x_start)};
+    }
+    return {0, 16, 0, 0};
+}
+
 template <class D, bool VISC, bool MIXED = false, bool TAB = true>
 struct Plan {
     // master tables (loaded once per CTA; shapvt / shapvg stay in global memory when !TAB)
@@ -144,19 +163,9 @@ struct Plan {
     static constexpr int TC_G = (D::NU + 7) / 8;                          // row groups of A with real rows
     static constexpr int TC_NP = (D::NH + 15) / 16 * 16;                  // right-hand sides, padded
     static constexpr int TC_ADBL = 2 * TC_G * TC_KC * 128 / 8;            // A hi + lo, in doubles
-    static constexpr int TC_BDBL = 2 * 2 * TC_KC * 128 / 8;               // one 16-row B tile, hi + lo
     static constexpr int inv_lo = INV_ALIAS ? d_inv : x_end, inv_hi = INV_ALIAS ? d_inv + D::NU * D::NU : x_end;
-    // free ranges [x_start, inv_lo) and [inv_hi, x_end) (offsets rounded up to 128 bytes): A and B
-    // in the upper one (1), or A in the lower and B in the upper one (2), or the reverse (3)
-    static constexpr int TC_PL =
-        !MIXED ? 0
-               : (al16(al16(inv_hi) + TC_ADBL) + TC_BDBL <= x_end
-                      ? 1
-                      : (al16(x_start) + TC_ADBL <= inv_lo && al16(inv_hi) + TC_BDBL <= x_end
-                             ? 2
-                             : (al16(inv_hi) + TC_ADBL <= x_end && al16(x_start) + TC_BDBL <= inv_lo ? 3 : 0)));
-    static constexpr int tc_a = TC_PL == 1 ? al16(inv_hi) : (TC_PL == 2 ? al16(x_start) : al16(inv_hi));
-    static constexpr int tc_b = TC_PL == 1 ? al16(tc_a + TC_ADBL) : (TC_PL == 2 ? al16(inv_hi) : al16(x_start));
+    static constexpr TcPlace TCP = tc_place(MIXED, x_start, inv_lo, inv_hi, x_end, TC_ADBL, TC_KC, TC_NP);
+    static constexpr int TC_PL = TCP.pl, TC_NB = TCP.nb, tc_a = TCP.a, tc_b = TCP.b;
     static constexpr bool TC = TC_PL != 0 && tc_a * 8 + 16 * TC_KC * 128 <= (int)(sizeof(double) * n_doubles) &&
                                TC_NP <= 256 && D::NU <= 64;
     // integers after the doubles
@@ -199,6 +208,9 @@ constexpr int cta_threads() {
 // is then refined against the FP64 SD to FP64 accuracy, and every residual (Ru, Rq, Rh, FE)
 // is FP64.  AE and DUDG_DUH therefore carry FP32-level errors (a Jacobian error, which
 // changes the Newton convergence rate, not the converged solution).
+// Tensor-core Schur product also in plans that run several CTAs per SM (see USE_TC below).
+constexpr bool kTcMultiCta = false;
+
 template <class D, bool VISC, bool MIXED, int NT>
 __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_kernel(const __grid_constant__ ElemParams P) {
     using L = PlanSel<D, VISC, MIXED>;
@@ -234,10 +246,15 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     for (int i = tid; i < NPF * NFE; i += NT) invp[perm[i] + NPV * (i / NPF)] = i % NPF;
     // mixed form: the tensor-memory accumulator of the Schur product and its mbarrier, once per CTA
     constexpr uint32_t TC_COLS = L::TC_NP <= 32 ? 32 : (L::TC_NP <= 64 ? 64 : (L::TC_NP <= 128 ? 128 : 256));
+    // Kernels that hold tensor memory run one CTA per SM (the runtime limits a TMEM-allocating
+    // kernel's occupancy to 1), while the smaller plans run three or four elements per SM and
+    // are bound by the latency of their elimination chain: the tensor-core Schur product is used
+    // where the plan runs one CTA per SM anyway (3D p = 2).
+    constexpr bool USE_TC = L::TC && (min_blocks<D, VISC, MIXED>() == 1 || kTcMultiCta);
     uint64_t *s_mbar = reinterpret_cast<uint64_t *>(sm + L::d_mbar);
     uint32_t tmem = 0, tc_phase = 0;
-    if constexpr (L::TC) {
-        if (tid < 32) tc::tmem_alloc(reinterpret_cast<uint32_t *>(si + L::i_tmem), TC_COLS);
+    if constexpr (USE_TC) {
+        if (tid < 32) tc::tmem_alloc<TC_COLS>(reinterpret_cast<uint32_t *>(si + L::i_tmem));
         if (tid == 0) {
             tc::mbar_init(s_mbar, 1);
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -245,7 +262,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         tc::fence_before_sync();
     }
     __syncthreads();
-    if constexpr (L::TC) {
+    if constexpr (USE_TC) {
         tc::fence_after_sync();
         tmem = *reinterpret_cast<const uint32_t *>(si + L::i_tmem);
     }
@@ -792,7 +809,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                 // [SD | r0 | I] only, the other right-hand sides are multiplied by SD^-1 below),
                 // then the residual column refined in FP64 against the FP64 SD with the FP32 inverse
                 double *s_inv = sm + L::d_inv;
-                gj_regs_nopiv_t<float, NU, L::TC ? 1 : 1 + NH, NU, true, NT, 8, NPV>(
+                gj_regs_nopiv_t<float, NU, USE_TC ? 1 : 1 + NH, NU, true, NT, 8, NPV>(
                     s_SD, s_R, s_inv, reinterpret_cast<float *>(s_pcol), s_bad);
                 double *s_res = s_pcol;                    // free after the elimination
                 for (int it = 0; it < 3; it++) {
@@ -870,15 +887,15 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             }
             if (tid == 0 && *s_bad && !bad_before) *s_bad = 2;
             __syncthreads();
-            if constexpr (L::TC) {
+            if constexpr (USE_TC) {
                 // Schur product on the tensor cores (tcgen05 kind::tf32, 3xTF32 with FP32
                 // accumulation): R(:, 1:) = SD^-1 R(:, 1:) (schur_primal.m:118, dlu = SD \ (BMiE - F)),
                 // once the residual column has passed its check (a pivoted redo solves R in FP64).
                 // A = SD^-1 (K-major: row r, column k), B = 16 right-hand sides per MMA round (row n
                 // = right-hand side, K-major), D = A B^T in TMEM columns n0 .. n0 + 15.
                 if (tc_go) {
-                    constexpr int KP = L::TC_KP, KC = L::TC_KC, GR = 8 * L::TC_G, NP = L::TC_NP;
-                    constexpr int AH = L::TC_G * KC * 128, BH = 2 * KC * 128;    // bytes of one hi / lo half
+                    constexpr int KP = L::TC_KP, KC = L::TC_KC, GR = 8 * L::TC_G, NP = L::TC_NP, NB = L::TC_NB;
+                    constexpr int AH = L::TC_G * KC * 128, BH = (NB / 8) * KC * 128;   // bytes of one hi / lo half
                     const double *s_inv = sm + L::d_inv;
                     unsigned char *tA = reinterpret_cast<unsigned char *>(sm + L::tc_a);
                     unsigned char *tB = reinterpret_cast<unsigned char *>(sm + L::tc_b);
@@ -890,11 +907,11 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                         *reinterpret_cast<float *>(tA + off) = h;
                         *reinterpret_cast<float *>(tA + AH + off) = l;
                     }
-                    constexpr uint32_t idesc = tc::idesc_tf32(128, 16);
+                    constexpr uint32_t idesc = tc::idesc_tf32(128, NB);
                     const uint32_t aaddr = tc::smem_u32(tA), baddr = tc::smem_u32(tB);
-                    for (int n0 = 0; n0 < NP; n0 += 16) {
-                        for (int i = tid; i < 16 * KP; i += NT) {
-                            const int n = i % 16, k = i / 16;
+                    for (int n0 = 0; n0 < NP; n0 += NB) {
+                        for (int i = tid; i < NB * KP; i += NT) {
+                            const int n = i % NB, k = i / NB;
                             float h = 0.f, l = 0.f;
                             if (n0 + n < NH && k < NU) tc::split_tf32(s_R[k + NU * (1 + n0 + n)], h, l);
                             const int off = tc::kmajor_offset(n, k, KC);
@@ -1062,7 +1079,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         if (tid == 0 && P.status) P.status[e] = *s_bad;
         __syncthreads();
     }
-    if constexpr (L::TC) {
+    if constexpr (USE_TC) {
         tc::fence_before_sync();
         __syncthreads();
         if (tid < 32) tc::tmem_dealloc(tmem, TC_COLS);

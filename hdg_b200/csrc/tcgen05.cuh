@@ -54,10 +54,12 @@ __device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
     lo = to_tf32(f - hi);
 }
 
-// ---- TMEM allocation: one warp, power-of-two column count in [32, 512]
-__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {
+// ---- TMEM allocation: one warp, power-of-two column count in [32, 512] (an immediate)
+template <uint32_t NCOLS>
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot) {
+    static_assert(NCOLS >= 32 && NCOLS <= 512 && (NCOLS & (NCOLS - 1)) == 0, "TMEM columns");
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
-                 "r"(ncols)
+                 "n"(NCOLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
 }

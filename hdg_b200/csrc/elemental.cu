@@ -65,21 +65,25 @@ constexpr int al16(int x) { return (x + 15) / 16 * 16; }   // a double offset ro
 
 // Placement of the tensor-core operands of the mixed form in the free scratch ranges
 // [x_start, inv_lo) and [inv_hi, x_end) (double offsets): A (SD^-1, adbl doubles) and a B tile of
-// nb right-hand sides (nb a multiple of 16 dividing np, as large as fits: fewer MMA rounds).
-// pl 0: no placement.
+// nbuf B tiles of nb right-hand sides each (nb a multiple of 16 dividing np).  Two tiles (the
+// next one is staged while the tensor core multiplies the current one) are preferred to a wider
+// single tile; among those, the widest nb that fits (fewer MMA rounds).  pl 0: no placement.
 struct TcPlace {
-    int pl, nb, a, b;
+    int pl, nb, nbuf, a, b;
 };
 constexpr TcPlace tc_place(bool mixed, int x_start, int inv_lo, int inv_hi, int x_end, int adbl, int kc, int np) {
-    if (!mixed) return {0, 16, 0, 0};
-    for (int nb = np; nb >= 16; nb -= 16) {
-        if (np % nb || nb > 256) continue;
-        const int bdbl = 2 * (nb / 8) * kc * 128 / 8;
-        if (al16(al16(inv_hi) + adbl) + bdbl <= x_end) return {1, nb, al16(inv_hi), al16(al16(inv_hi) + adbl)};
-        if (al16(x_start) + adbl <= inv_lo && al16(inv_hi) + bdbl <= x_end) return {2, nb, al16(x_start), al16(inv_hi)};
-        if (al16(inv_hi) + adbl <= x_end && al16(x_start) + bdbl <= inv_lo) return {3, nb, al16(inv_hi), al16(x_start)};
-    }
-    return {0, 16, 0, 0};
+    if (!mixed) return {0, 16, 1, 0, 0};
+    for (int nbuf = 2; nbuf >= 1; nbuf--)
+        for (int nb = np; nb >= 16; nb -= 16) {
+            if (np % nb || nb > 256 || (nbuf == 2 && nb == np && np > 16)) continue;   // two buffers need two rounds
+            const int bdbl = nbuf * al16(2 * (nb / 8) * kc * 128 / 8);
+            if (al16(al16(inv_hi) + adbl) + bdbl <= x_end) return {1, nb, nbuf, al16(inv_hi), al16(al16(inv_hi) + adbl)};
+            if (al16(x_start) + adbl <= inv_lo && al16(inv_hi) + bdbl <= x_end)
+                return {2, nb, nbuf, al16(x_start), al16(inv_hi)};
+            if (al16(inv_hi) + adbl <= x_end && al16(x_start) + bdbl <= inv_lo)
+                return {3, nb, nbuf, al16(inv_hi), al16(x_start)};
+        }
+    return {0, 16, 1, 0, 0};
 }
 
 template <class D, bool VISC, bool MIXED = false, bool TAB = true>
@@ -150,7 +154,7 @@ struct Plan {
     static constexpr int d_b0 = d_diag + D::NU;                         // [NU] first right-hand side
     static constexpr int d_invsep = d_b0 + D::NU;                       // [NU*NU] FP32-accurate SD^-1 (MIXED)
     static constexpr int d_mbar = d_invsep + ((MIXED && !INV_ALIAS) ? D::NU * D::NU : 0);   // tensor-core mbarrier
-    static constexpr int n_doubles = d_mbar + (MIXED ? 2 : 0);
+    static constexpr int n_doubles = d_mbar + (MIXED ? 4 : 0);                    // two mbarriers (16-byte slot each)
     static constexpr int d_inv = INV_ALIAS ? x_start + (SD_ALIAS ? D::NU * D::NU : 0) : d_invsep;
     // Tensor-core Schur product of the mixed form, X = SD^-1 [B Mi E - F] (tcgen05, 3xTF32): the
     // operands, SD^-1 as A (M = 128 rows of which NU are real, K = NU padded to the MMA step) and
@@ -165,7 +169,8 @@ struct Plan {
     static constexpr int TC_ADBL = 2 * TC_G * TC_KC * 128 / 8;            // A hi + lo, in doubles
     static constexpr int inv_lo = INV_ALIAS ? d_inv : x_end, inv_hi = INV_ALIAS ? d_inv + D::NU * D::NU : x_end;
     static constexpr TcPlace TCP = tc_place(MIXED, x_start, inv_lo, inv_hi, x_end, TC_ADBL, TC_KC, TC_NP);
-    static constexpr int TC_PL = TCP.pl, TC_NB = TCP.nb, tc_a = TCP.a, tc_b = TCP.b;
+    static constexpr int TC_PL = TCP.pl, TC_NB = TCP.nb, TC_NBUF = TCP.nbuf, tc_a = TCP.a, tc_b = TCP.b;
+    static constexpr int TC_BSTRIDE = al16(2 * (TC_NB / 8) * TC_KC * 128 / 8);   // doubles between B tiles
     static constexpr bool TC = TC_PL != 0 && tc_a * 8 + 16 * TC_KC * 128 <= (int)(sizeof(double) * n_doubles) &&
                                TC_NP <= 256 && D::NU <= 64;
     // integers after the doubles
@@ -252,11 +257,12 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     // where the plan runs one CTA per SM anyway (3D p = 2).
     constexpr bool USE_TC = L::TC && (min_blocks<D, VISC, MIXED>() == 1 || kTcMultiCta);
     uint64_t *s_mbar = reinterpret_cast<uint64_t *>(sm + L::d_mbar);
-    uint32_t tmem = 0, tc_phase = 0;
+    uint32_t tmem = 0, tc_phases = 0;          // bit b: the phase parity mbarrier b waits for next
     if constexpr (USE_TC) {
         if (tid < 32) tc::tmem_alloc<TC_COLS>(reinterpret_cast<uint32_t *>(si + L::i_tmem));
         if (tid == 0) {
             tc::mbar_init(s_mbar, 1);
+            tc::mbar_init(s_mbar + 2, 1);
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
         tc::fence_before_sync();
@@ -908,20 +914,33 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                         *reinterpret_cast<float *>(tA + AH + off) = l;
                     }
                     constexpr uint32_t idesc = tc::idesc_tf32(128, NB);
-                    const uint32_t aaddr = tc::smem_u32(tA), baddr = tc::smem_u32(tB);
-                    for (int n0 = 0; n0 < NP; n0 += NB) {
+                    constexpr int NBUF = L::TC_NBUF, NROUND = NP / NB;
+                    const uint32_t aaddr = tc::smem_u32(tA);
+                    // round r stages its B tile in buffer r % NBUF and multiplies it into TMEM columns
+                    // r NB ..; buffer b's mbarrier completes once that buffer's MMAs are done, and a
+                    // buffer is rewritten only after its previous round's MMAs have completed, so
+                    // staging round r + 1 overlaps the tensor core's work on round r
+                    for (int r = 0; r < NROUND; r++) {
+                        const int b = r % NBUF, n0 = r * NB;
+                        unsigned char *tb = tB + (size_t)8 * L::TC_BSTRIDE * b;
+                        if (r >= NBUF) {
+                            if (!tc::mbar_wait(s_mbar + 2 * b, (tc_phases >> b) & 1u, 1 << 22)) *s_bad = 4;
+                            tc_phases ^= 1u << b;
+                            tc::fence_after_sync();
+                        }
                         for (int i = tid; i < NB * KP; i += NT) {
                             const int n = i % NB, k = i / NB;
                             float h = 0.f, l = 0.f;
                             if (n0 + n < NH && k < NU) tc::split_tf32(s_R[k + NU * (1 + n0 + n)], h, l);
                             const int off = tc::kmajor_offset(n, k, KC);
-                            *reinterpret_cast<float *>(tB + off) = h;
-                            *reinterpret_cast<float *>(tB + BH + off) = l;
+                            *reinterpret_cast<float *>(tb + off) = h;
+                            *reinterpret_cast<float *>(tb + BH + off) = l;
                         }
                         tc::fence_proxy_async();
                         __syncthreads();
                         if (tid == 0) {
                             tc::fence_after_sync();
+                            const uint32_t baddr = tc::smem_u32(tb);
 #pragma unroll
                             for (int s = 0; s < KP / 8; s++) {
                                 const uint64_t ah = tc::smem_desc(aaddr + 256 * s, 128, KC * 128);
@@ -932,13 +951,15 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                                 tc::mma_tf32(tmem + n0, ah, bl, idesc, true);
                                 tc::mma_tf32(tmem + n0, ah, bh, idesc, true);
                             }
-                            tc::commit(s_mbar);
+                            tc::commit(s_mbar + 2 * b);
                         }
-                        // every thread sees the MMAs complete before the next round rewrites B
-                        if (!tc::mbar_wait(s_mbar, tc_phase, 1 << 22)) *s_bad = 4;
-                        tc_phase ^= 1;
-                        tc::fence_after_sync();
                     }
+                    // the last round of every buffer
+                    for (int b = 0; b < NBUF && b < NROUND; b++) {
+                        if (!tc::mbar_wait(s_mbar + 2 * b, (tc_phases >> b) & 1u, 1 << 22)) *s_bad = 4;
+                        tc_phases ^= 1u << b;
+                    }
+                    tc::fence_after_sync();
                     // rows r < NU are TMEM lanes 0..NU-1: warp w reads lanes 32 w .. 32 w + 31
                     if (tid < 32 * ((NU + 31) / 32)) {
                         const int w = tid >> 5;

@@ -65,17 +65,18 @@ constexpr int al16(int x) { return (x + 15) / 16 * 16; }   // a double offset ro
 
 // Placement of the tensor-core operands of the mixed form in the free scratch ranges
 // [x_start, inv_lo) and [inv_hi, x_end) (double offsets): A (SD^-1, adbl doubles) and a B tile of
-// nbuf B tiles of nb right-hand sides each (nb a multiple of 16 dividing np).  Two tiles (the
-// next one is staged while the tensor core multiplies the current one) are preferred to a wider
-// single tile; among those, the widest nb that fits (fewer MMA rounds).  pl 0: no placement.
+// nbuf B tiles of nb right-hand sides each (nb a multiple of 16 dividing np).  The widest nb
+// that fits is taken (every MMA round costs two CTA barriers and a proxy fence; measured on 3D
+// p = 2: four rounds of 32 right-hand sides beat eight double-buffered rounds of 16), with a
+// second buffer when two tiles of that width fit.  pl 0: no placement.
 struct TcPlace {
     int pl, nb, nbuf, a, b;
 };
 constexpr TcPlace tc_place(bool mixed, int x_start, int inv_lo, int inv_hi, int x_end, int adbl, int kc, int np) {
     if (!mixed) return {0, 16, 1, 0, 0};
-    for (int nbuf = 2; nbuf >= 1; nbuf--)
-        for (int nb = np; nb >= 16; nb -= 16) {
-            if (np % nb || nb > 256 || (nbuf == 2 && nb == np && np > 16)) continue;   // two buffers need two rounds
+    for (int nb = np; nb >= 16; nb -= 16)
+        for (int nbuf = 2; nbuf >= 1; nbuf--) {
+            if (np % nb || nb > 256 || (nbuf == 2 && nb == np)) continue;   // two buffers need two rounds
             const int bdbl = nbuf * al16(2 * (nb / 8) * kc * 128 / 8);
             if (al16(al16(inv_hi) + adbl) + bdbl <= x_end) return {1, nb, nbuf, al16(inv_hi), al16(al16(inv_hi) + adbl)};
             if (al16(x_start) + adbl <= inv_lo && al16(inv_hi) + bdbl <= x_end)

@@ -129,12 +129,17 @@ def latency_stats(reqs, t0):
 
 
 class Server:
-    def __init__(self, slots=8, memory_budget=None, ordering="multicolor", mixed=False, restart=20, engine="native"):
+    def __init__(self, slots=8, memory_budget=None, ordering="multicolor", mixed=False, restart=20, engine="native",
+                 max_bypass=4):
+        """max_bypass: how many later requests may be admitted ahead of a waiting request that
+        does not fit yet (a large request waiting for memory does not block small ones behind
+        it, but it is not overtaken more than this many times)."""
         if memory_budget is None:
             free, _ = torch.cuda.mem_get_info()
             memory_budget = int(0.8 * free)
         self.slots, self.budget = slots, memory_budget
         self.ordering, self.mixed, self.restart, self.engine = ordering, mixed, restart, engine
+        self.max_bypass = max_bypass
 
     def serve(self, reqs, realtime=True):
         """Run the requests with continuous admission; returns latency statistics."""
@@ -168,17 +173,36 @@ class Server:
         if not realtime:
             for r in pending:
                 r.arrival = 0.0
+        fps = {r.rid: footprint_bytes(r.problem, self.restart) for r in pending}
+        bypassed = {r.rid: 0 for r in pending}
+
+        def pick(t):
+            """Index of the request to admit now, or None: the earliest arrived request that
+            fits, unless an earlier one that does not fit has been overtaken max_bypass times."""
+            if not free_streams:
+                return None
+            for i, r in enumerate(pending):
+                if r.arrival > t:
+                    return None
+                if state["used"] + fps[r.rid] <= self.budget or state["running"] == 0:
+                    return i
+                if bypassed[r.rid] >= self.max_bypass:
+                    return None
+            return None
+
         while pending:
-            req = pending[0]
-            fp = footprint_bytes(req.problem, self.restart)
             with lock:
                 while True:
-                    wait_arrival = req.arrival - now()
-                    fits = state["used"] + fp <= self.budget or state["running"] == 0
-                    if wait_arrival <= 0 and free_streams and fits:
+                    t = now()
+                    i = pick(t)
+                    if i is not None:
                         break
-                    lock.wait(timeout=max(1e-3, min(wait_arrival, 0.05)) if wait_arrival > 0 else 0.05)
-                pending.pop(0)
+                    nxt = [r.arrival - t for r in pending if r.arrival > t]
+                    lock.wait(timeout=max(1e-3, min(min(nxt), 0.05)) if nxt else 0.05)
+                req = pending.pop(i)
+                for r in pending[:i]:
+                    bypassed[r.rid] += 1
+                fp = fps[req.rid]
                 sid = free_streams.pop(0)
                 state["used"] += fp
                 state["running"] += 1

@@ -41,3 +41,32 @@ def test_admission_under_tight_memory_budget():
     spans = sorted((r.admitted, r.finished) for r in reqs)
     for (a0, f0), (a1, f1) in zip(spans, spans[1:]):
         assert a1 >= f0 - 1e-3
+
+
+def _bypass_mix():
+    """A small request, then a large one, then two small ones, all queued at t = 0."""
+    from hdg_b200.serve import request_mix
+    small = request_mix(5, 3, nmin=4, nmax=4, pmin=1, pmax=1, rate=50.0)
+    big = request_mix(6, 1, nmin=12, nmax=12, pmin=3, pmax=3, rate=50.0)[0]
+    reqs = [small[0], big, small[1], small[2]]
+    for i, r in enumerate(reqs):
+        r.rid = i
+    return reqs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("max_bypass", [0, 4])
+def test_admission_past_a_request_that_does_not_fit(max_bypass):
+    """With memory for the large request alone (or for the small ones together), the small
+    requests behind it are admitted while it waits, unless bypassing is switched off."""
+    from hdg_b200.serve import Server, footprint_bytes
+    reqs = _bypass_mix()
+    fp = [footprint_bytes(r.problem) for r in reqs]
+    assert fp[0] + fp[2] + fp[3] <= fp[1]
+    stats = Server(slots=4, memory_budget=fp[1], max_bypass=max_bypass).serve(reqs, realtime=False)
+    assert stats["converged"] == 4
+    big, s1 = reqs[1], reqs[2]
+    if max_bypass:
+        assert s1.admitted < big.admitted
+    else:
+        assert big.admitted <= s1.admitted

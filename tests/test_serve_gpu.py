@@ -47,7 +47,7 @@ def _bypass_mix():
     """A small request, then a large one, then two small ones, all queued at t = 0."""
     from hdg_b200.serve import request_mix
     small = request_mix(5, 3, nmin=4, nmax=4, pmin=1, pmax=1, rate=50.0)
-    big = request_mix(6, 1, nmin=12, nmax=12, pmin=3, pmax=3, rate=50.0)[0]
+    big = request_mix(6, 1, nmin=30, nmax=30, pmin=4, pmax=4, rate=50.0)[0]
     reqs = [small[0], big, small[1], small[2]]
     for i, r in enumerate(reqs):
         r.rid = i

@@ -51,6 +51,7 @@ def _bypass_mix():
     reqs = [small[0], big, small[1], small[2]]
     for i, r in enumerate(reqs):
         r.rid = i
+        r.arrival = 1e-3 * i          # this order (the server sorts by arrival, then zeroes it)
     return reqs
 
 

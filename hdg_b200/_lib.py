@@ -142,6 +142,21 @@ def _declare(L):
     L.hdgx_solve.argtypes = [p(HdgxMaster), p(HdgxApp), p(HdgxMesh), v, v, v, p(HdgxSolveOpts), p(HdgxSolveReport), v]
     L.hdgx_elemental_buckets.restype = i
     L.hdgx_elemental_buckets.argtypes = [i, v, i, v]
+    L.hdgx_elemental_shared.restype = i
+    L.hdgx_elemental_shared.argtypes = [i, v, i, v]
+    L.hdgx_elemental_shared_max.restype = i
+    L.hdgx_elemental_shared_max.argtypes = []
+    L.hdgx_combiner_create.restype = i
+    L.hdgx_combiner_create.argtypes = [i, p(v)]
+    L.hdgx_combiner_destroy.restype = i
+    L.hdgx_combiner_destroy.argtypes = [v]
+    L.hdgx_combiner_stats.restype = i
+    L.hdgx_combiner_stats.argtypes = [v, p(ct.c_longlong), p(ct.c_longlong), p(ct.c_longlong)]
+    L.hdgx_combiner_times.restype = i
+    L.hdgx_combiner_times.argtypes = [v, p(d), p(d)]
+    L.hdgx_solve_combined.restype = i
+    L.hdgx_solve_combined.argtypes = [p(HdgxMaster), p(HdgxApp), p(HdgxMesh), v, v, v, p(HdgxSolveOpts),
+                                      p(HdgxSolveReport), v, v]
     L.hdgx_arraymul.restype = i
     L.hdgx_arraymul.argtypes = [i, i, i, i, i, i, v, v, v, v]
     L.hdgx_dense_block_system.restype = i

@@ -6,6 +6,10 @@ concurrently on forked side streams; capturable as one CUDA graph with ``capture
 ``replay()``), or degree by degree on one stream (``run_sequential``, the plain per-degree
 launches).  Outputs are identical bit for bit either way: every element's arithmetic is the
 same, only the launch schedule differs.
+
+``SharedLaunch`` evaluates several independent problems of one element shape (e.g. the
+same-degree requests of a serving mix, each with its own physics) as ONE segmented launch
+(``hdgx_elemental_shared``), or problem by problem (``run_each``), with identical outputs.
 """
 from __future__ import annotations
 
@@ -86,3 +90,49 @@ class ElementalBuckets:
 
     def statuses(self):
         return [int(b["out"].status.numpy().max()) if b["ne"] else 0 for b in self.buckets]
+
+
+class SharedLaunch:
+    """Several problems of one (nd, porder) and one physics kind in one elemental launch."""
+
+    def __init__(self, problems):
+        _require_cuda()
+        self.items = []
+        for P in problems:
+            m = P.mesh
+            it = dict(P=P, ne=int(m.ne), dm=DeviceMaster(P.master), appc=app_struct(P.app),
+                      dg=DArray.from_numpy(m.dgnodes), bf=DArray.from_numpy(m.bf, dtype=torch.int32),
+                      udg=DArray.from_numpy(P.UDG), uh=DArray.from_numpy(P.uh_elem()), sh=DArray.from_numpy(P.SH))
+            it["out"] = alloc_elemental_outputs(P.master, P.app, it["ne"])
+            self.items.append(it)
+        arr = (HdgxElemBucket * len(self.items))()
+        for k, it in enumerate(self.items):
+            o = it["out"]
+            arr[k] = HdgxElemBucket(ct.addressof(it["dm"].c), ct.addressof(it["appc"]), it["ne"], it["dg"].ptr,
+                                    it["bf"].ptr, it["udg"].ptr, it["uh"].ptr, it["sh"].ptr, o.AE.ptr, o.FE.ptr,
+                                    o.DUDG.ptr, o.DUDG_DUH.ptr, o.status.ptr, 0)
+        self._arr = arr
+
+    @property
+    def ne(self):
+        return sum(it["ne"] for it in self.items)
+
+    def run(self, grid=0, stream=None):
+        """One launch over every problem's elements (status -2: shapes or physics kinds differ)."""
+        rc = lib().hdgx_elemental_shared(len(self.items), ct.cast(self._arr, ct.c_void_p), int(grid),
+                                         _stream_ptr(stream))
+        check(rc, "hdgx_elemental_shared")
+
+    def run_each(self, stream=None):
+        """One hdgx_elemental launch per problem, one after another."""
+        L = lib()
+        for it in self.items:
+            o = it["out"]
+            rc = L.hdgx_elemental(ct.byref(it["dm"].c), ct.byref(it["appc"]), it["ne"], it["dg"].ptr, it["bf"].ptr,
+                                  it["udg"].ptr, it["uh"].ptr, it["sh"].ptr, o.AE.ptr, o.FE.ptr, o.DUDG.ptr,
+                                  o.DUDG_DUH.ptr, o.status.ptr, _stream_ptr(stream))
+            check(rc, "hdgx_elemental")
+
+    def outputs(self):
+        return [[getattr(it["out"], k).numpy().copy() for k in ("AE", "FE", "DUDG", "DUDG_DUH", "status")]
+                for it in self.items]

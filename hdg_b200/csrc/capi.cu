@@ -11,6 +11,8 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
                      int grid, double *QDG = nullptr, double *RU = nullptr);
 cudaMemPool_t device_pool();
 int elemental_check_master(const hdgx_master *m);
+int elemental_launch_shared(int nb, const hdgx_elem_bucket *b, cudaStream_t st, int grid);
+int elemental_shared_max_segments();
 int schur_adjoint_launch(int qform, int nd, int npv, int ncu, int nc, int ndf, int ne, const double *M,
                          const double *C, const double *E, const double *BD, const double *F, const double *GK,
                          const double *H, const double *Rq, const double *Ru, const double *Rh, double *DUDG,
@@ -207,6 +209,21 @@ int hdgx_elemental_buckets(int nb, const hdgx_elem_bucket *b, int mixed, hdgx_st
     }
     return rc;
 }
+
+int hdgx_elemental_shared(int nb, const hdgx_elem_bucket *b, int grid, hdgx_stream_t stream) {
+    if (nb < 0 || (nb > 0 && !b) || grid < 0) return -1;
+    if (nb == 0) return 0;
+    if (nb > hdgx::elemental_shared_max_segments()) return -5;
+    for (int k = 0; k < nb; k++) {
+        const hdgx_elem_bucket &q = b[k];
+        if (int rc = check_elemental(q.master, q.app, q.ne, q.dgnodes, q.bf, q.UDG, q.UH, q.SH, q.AE, q.FE, q.DUDG,
+                                     q.DUDG_DUH))
+            return rc;
+    }
+    return hdgx::elemental_launch_shared(nb, b, (cudaStream_t)stream, grid);
+}
+
+int hdgx_elemental_shared_max(void) { return hdgx::elemental_shared_max_segments(); }
 
 // Host-array form: the elements go through two device staging sets in chunks, and chunk c's
 // upload (stream s_in), chunk c-1's kernel (the caller's stream) and chunk c-2's download

@@ -45,6 +45,25 @@ struct ElemParams {
     double *RU;                // non-NULL: residual mode (kernel/cuda_residual.m), Ru at q = getq(u, uh)
 };
 
+// One launch over the same-shape elements of several independent element sets (e.g. of several
+// serving requests): segment s is seg[s]'s arrays and physics, its elements are
+// [seg_start[s], seg_start[s + 1]) of the launch; the master tables are seg[0]'s.  The table is the
+// kernel's parameter (up to 32 KB of parameters on sm_70+ with CUDA 12.1+), so a launch needs no
+// upload and is captured into a CUDA graph like any other.
+constexpr int kMaxSeg = 24;
+struct SegTable {
+    ElemParams seg[kMaxSeg];
+    int seg_start[kMaxSeg + 1];
+    int nseg;
+};
+static_assert(sizeof(SegTable) < 32000, "kernel parameter limit");
+
+// The launch's base parameters (the master tables) and its element count
+__device__ __forceinline__ const ElemParams &base_params(const ElemParams &A) { return A; }
+__device__ __forceinline__ const ElemParams &base_params(const SegTable &A) { return A.seg[0]; }
+__device__ __forceinline__ int launch_ne(const ElemParams &A) { return A.ne; }
+__device__ __forceinline__ int launch_ne(const SegTable &A) { return A.seg_start[A.nseg]; }
+
 template <int ND_, int NPV_, int NPF_, int NGV_, int NGF_>
 struct Dims {
     static constexpr int ND = ND_, NPV = NPV_, NPF = NPF_, NGV = NGV_, NGF = NGF_;
@@ -217,8 +236,10 @@ constexpr int cta_threads() {
 // Tensor-core Schur product also in plans that run several CTAs per SM (see USE_TC below).
 constexpr bool kTcMultiCta = false;
 
-template <class D, bool VISC, bool MIXED, int NT>
-__global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_kernel(const __grid_constant__ ElemParams P) {
+template <class D, bool VISC, bool MIXED, int NT, class Arg = ElemParams>
+__global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_kernel(const __grid_constant__ Arg A) {
+    constexpr bool SEG = !std::is_same<Arg, ElemParams>::value;
+    const ElemParams &P = base_params(A);
     using L = PlanSel<D, VISC, MIXED>;
     constexpr int ND = D::ND, NPV = D::NPV, NPF = D::NPF, NGV = D::NGV, NGF = D::NGF;
     constexpr int NFE = D::NFE, NCU = D::NCU, NC = D::NC, NDF = D::NDF, NU = D::NU;
@@ -290,19 +311,29 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     unsigned long long *s_slot = reinterpret_cast<unsigned long long *>(sm + L::d_slots);
     double *s_pcol = sm + L::d_pcol, *s_diag = sm + L::d_diag;
 
-    for (int e = blockIdx.x; e < P.ne; e += gridDim.x) {
+    int seg = 0;                                 // segmented launches: the segment of element eg
+    const int ne_launch = launch_ne(A);
+    for (int eg = blockIdx.x; eg < ne_launch; eg += gridDim.x) {
+        const ElemParams *Qp = &P;
+        int e = eg;
+        if constexpr (SEG) {
+            while (eg >= A.seg_start[seg + 1]) seg++;
+            Qp = &A.seg[seg];
+            e = eg - A.seg_start[seg];
+        }
+        const ElemParams &Q = *Qp;   // this element's arrays and physics
         bool force_piv = false;      // set when the unpivoted solve failed its check and SD sits on
                                      // the scratch: the element is then evaluated again, pivoted
     elem_start:
         // ================================================================ load
         {
-            const double *g_dg = P.dgnodes + (size_t)e * NPV * ND;
-            const double *g_udg = P.UDG + (size_t)e * NPV * NC;
-            const double *g_uh = P.UH + (size_t)e * NCU * NDF;
+            const double *g_dg = Q.dgnodes + (size_t)e * NPV * ND;
+            const double *g_udg = Q.UDG + (size_t)e * NPV * NC;
+            const double *g_uh = Q.UH + (size_t)e * NCU * NDF;
             for (int i = tid; i < NPV * ND; i += NT) s_dg[i] = g_dg[i];
             for (int i = tid; i < NPV * NC; i += NT) s_udg[i] = g_udg[i];
             for (int i = tid; i < NCU * NDF; i += NT) s_uh[i] = g_uh[i];
-            if (tid < NFE) s_bf[tid] = P.bf[(size_t)e * NFE + tid];
+            if (tid < NFE) s_bf[tid] = Q.bf[(size_t)e * NFE + tid];
             if (tid == 0) *s_bad = 0;
         }
         __syncthreads();
@@ -400,7 +431,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             double t = 0.0;
 #pragma unroll
             for (int g = 0; g < NGV; g++) t += t_vg[r + NPV * g] * t_vt[g + NGV * s] * x_jac[g];
-            s_M[i] = P.fc_q * t;
+            s_M[i] = Q.fc_q * t;
         }
         if (tid < NGV) s_jv[tid] = x_jac[tid];
         for (int i = tid; i < NPV * NPV * ND; i += NT) {
@@ -430,15 +461,15 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         }
         __syncthreads();
         // Rq = M (SH/fc_q - q) + C u - E uh   (volint.m:57-60, faceint.m:49-51)
-        const double *__restrict__ g_shq = P.SH + (size_t)e * NPV * NC + NPV * NCU;   // q part of SH
+        const double *__restrict__ g_shq = Q.SH + (size_t)e * NPV * NC + NPV * NCU;   // q part of SH
         for (int i = tid; i < NPV * NCU * ND; i += NT) {
             const int r = i % NPV, a = (i / NPV) % NCU, d = i / (NPV * NCU);
             const int cq = NCU + a + NCU * d;
             double t = 0.0;
 #pragma unroll
             for (int s = 0; s < NPV; s++)
-                t += s_M[r + NPV * s] * ((P.SH ? g_shq[s + NPV * (a + NCU * d)] / P.fc_q : 0.0) -
-                                         ((P.QDG || P.RU) ? 0.0 : s_udg[s + NPV * cq]));   // getq: q does not enter
+                t += s_M[r + NPV * s] * ((Q.SH ? g_shq[s + NPV * (a + NCU * d)] / Q.fc_q : 0.0) -
+                                         ((Q.QDG || Q.RU) ? 0.0 : s_udg[s + NPV * cq]));   // getq: q does not enter
 #pragma unroll
             for (int s = 0; s < NPV; s++) t += s_MiC[r + NPV * (s + NPV * d)] * s_udg[s + NPV * a];
             for (int f = 0; f < NDF; f++) t -= s_MiE[r + NPV * (f + NDF * d)] * s_uh[a + NCU * f];
@@ -451,16 +482,16 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         gj_regs_nopiv<NPV, NPV * ND + NDF * ND + NCU * ND, NT, 8>(s_M, s_MiC, s_pcol, s_bad);
         if (tid == 0 && *s_bad) *s_bad = 1;
         __syncthreads();
-        if (P.QDG) {
+        if (Q.QDG) {
             // getq.m:37-104: the q that zeroes Rq for this u and uh; with q left out of Rq above,
             // Mi Rq = inv(fc_q Mu) (fc_q Mu SH_q / fc_q + C u - E uh)
-            double *g_q = P.QDG + (size_t)e * NPV * NCU * ND;
+            double *g_q = Q.QDG + (size_t)e * NPV * NCU * ND;
             for (int i = tid; i < NPV * NCU * ND; i += NT) g_q[i] = s_MiRq[i];
-            if (tid == 0 && P.status) P.status[e] = *s_bad;
+            if (tid == 0 && Q.status) Q.status[e] = *s_bad;
             __syncthreads();
             continue;
         }
-        if (P.RU) {
+        if (Q.RU) {
             // cuda_residual.m:3-4: q from getq, then the u residual is evaluated at that q; Rq is
             // zero at that q, so Mi Rq (and its Gauss-point values below) are set to exact zeros
             for (int i = tid; i < NPV * NCU * ND; i += NT) {
@@ -494,7 +525,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             for (int c = 0; c < NCU; c++) u[c] = {x_ug[g + NGV * c], c == sd ? 1.0 : 0.0};
 #pragma unroll
             for (int c = 0; c < NCU * ND; c++) q[c] = {x_ug[g + NGV * (NCU + c)], (NCU + c) == sd ? 1.0 : 0.0};
-            ns_flux<ND>(P.pc, u, q, f);
+            ns_flux<ND>(Q.pc, u, q, f);
 #pragma unroll
             for (int id = 0; id < ND; id++)
 #pragma unroll
@@ -521,14 +552,14 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             for (int c = 0; c < NCU; c++) u[c] = {x_fuh[gg + NGT * c], c == sd ? 1.0 : 0.0};
 #pragma unroll
             for (int c = 0; c < NCU * ND; c++) q[c] = {x_fu[gg + NGT * (NCU + c)], (NCU + c) == sd ? 1.0 : 0.0};
-            ns_flux<ND>(P.pc, u, q, f);
+            ns_flux<ND>(Q.pc, u, q, f);
             const double jc = x_jf[gg];
             const int j = gg / NGF;
             const int bnd = s_bf[j] < 0;
             const int ib = bnd ? -s_bf[j] - 1 : 0;
-            const int btype = bnd ? ((ib < P.nbnd) ? P.bcm[ib] : -1) : 0;
+            const int btype = bnd ? ((ib < Q.nbnd) ? Q.bcm[ib] : -1) : 0;
             const bool dir = bnd && btype == 6;                        // ns/fbou.m:111-114, both families
-            const bool per = bnd && btype == 5 && P.fb.fam == 0;       // ns/fbou.m:109-110: fhat
+            const bool per = bnd && btype == 5 && Q.fb.fam == 0;       // ns/fbou.m:109-110: fhat
             const bool gen = bnd && !dir && !per;                      // the other fbou.m types
 #pragma unroll
             for (int a = 0; a < NCU; a++) {
@@ -540,15 +571,15 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     dfn += f[a + NCU * jd].d * nl;
                 }
                 if (sd == 0) {
-                    const double fh = fn + P.pc.tau * (x_fu[gg + NGT * a] - x_fuh[gg + NGT * a]);
+                    const double fh = fn + Q.pc.tau * (x_fu[gg + NGT * a] - x_fuh[gg + NGT * a]);
                     x_FH[gg + NGT * a] = jc * fh;
-                    const double bh = dir ? (x_fuh[gg + NGT * a] - P.bcs[ib * 5 + a]) : fh;
+                    const double bh = dir ? (x_fuh[gg + NGT * a] - Q.bcs[ib * 5 + a]) : fh;
                     if (!gen) x_BH[gg + NGT * a] = jc * bh;
                 }
                 if (sd < NCU) {
                     // dfhat/duh (seed on uh) and dfhat/du = tau I
-                    const double fhh = dfn - (a == sd ? P.pc.tau : 0.0);
-                    const double fhu = (a == sd ? P.pc.tau : 0.0);
+                    const double fhh = dfn - (a == sd ? Q.pc.tau : 0.0);
+                    const double fhu = (a == sd ? Q.pc.tau : 0.0);
                     x_FHh[gg + NGT * (a + NCU * sd)] = jc * fhh;
                     x_FHu[gg + NGT * (a + NCU * sd)] = jc * fhu;
                     if (!gen) {
@@ -575,8 +606,8 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                 }
 #pragma unroll
                 for (int c = 0; c < NCU * ND; c++) qq[c] = {x_fu[gg + NGT * (NCU + c)], (NCU + c) == sd ? 1.0 : 0.0};
-                const double *ub = P.bcs + (ib < P.nbnd ? ib : 0) * 5;
-                if (!fbou_point<ND>(P.fb, P.pc, btype, ub, nlp, uu, qq, hh, fb)) *s_bad = 3;
+                const double *ub = Q.bcs + (ib < Q.nbnd ? ib : 0) * 5;
+                if (!fbou_point<ND>(Q.fb, Q.pc, btype, ub, nlp, uu, qq, hh, fb)) *s_bad = 3;
 #pragma unroll
                 for (int a = 0; a < NCU; a++) {
                     if (sd == 0) x_BH[gg + NGT * a] = jc * fb[a].v;
@@ -589,7 +620,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                         uu[c].d = c == sd ? 1.0 : 0.0;
                         hh[c].d = 0.0;
                     }
-                    fbou_point<ND>(P.fb, P.pc, btype, ub, nlp, uu, qq, hh, fb);
+                    fbou_point<ND>(Q.fb, Q.pc, btype, ub, nlp, uu, qq, hh, fb);
 #pragma unroll
                     for (int a = 0; a < NCU; a++) s_Gp[gg + NGT * (a + NCU * sd)] = jc * fb[a].d;
                 }
@@ -688,13 +719,13 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             },
             [&](int ab, int r, int k, double v) {
                 const int a = ab % NCU, b = ab / NCU;
-                if (P.tdep && a == b) {
+                if (Q.tdep && a == b) {
                     // time-dependent problems: the source Jacobian -fc_u on the u components
                     // (volint.m:215-216) enters BD, hence D, as fc_u * sum_g phi_r phi_k w_g jac_g
                     double mu = 0.0;
 #pragma unroll
                     for (int g = 0; g < NGV; g++) mu += t_vg[r + NPV * g] * t_vt[g + NGV * k] * s_jv[g];
-                    v += P.fc_u * mu;
+                    v += Q.fc_u * mu;
                 }
                 s_SD[(r + NPV * a) + NU * (k + NPV * b)] = v;
             });
@@ -728,15 +759,15 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     v += t_fg[m + NPF * g] * w;
                 }
             }
-            if (P.tdep) {
+            if (Q.tdep) {
                 // s = SH_u - fc_u u at the volume Gauss points, Ru += shapvg(:,:,1) (s jac)
                 // (volint.m:180-221 with dtcoef = 1 and no axisymmetry; volint.m:241,258)
-                const double *__restrict__ g_sh = P.SH ? P.SH + (size_t)e * NPV * NC + NPV * a : nullptr;
+                const double *__restrict__ g_sh = Q.SH ? Q.SH + (size_t)e * NPV * NC + NPV * a : nullptr;
                 for (int g = 0; g < NGV; g++) {
                     double st = 0.0;
 #pragma unroll
                     for (int s = 0; s < NPV; s++) st += t_vt[g + NGV * s] * (g_sh ? g_sh[s] : 0.0);
-                    v += t_vg[r + NPV * g] * ((st - x_ug[g + NGV * a] * P.fc_u) * s_jv[g]);
+                    v += t_vg[r + NPV * g] * ((st - x_ug[g + NGV * a] * Q.fc_u) * s_jv[g]);
                 }
             }
             s_R[i] = v;
@@ -776,11 +807,11 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             });
         };
         build_rhs();
-        if (P.RU) {
+        if (Q.RU) {
             // cuda_residual.m: the element u residual Ru (volume and face terms, time source)
             __syncthreads();
-            for (int i = tid; i < NU; i += NT) P.RU[(size_t)e * NU + i] = s_R[i];
-            if (tid == 0 && P.status) P.status[e] = *s_bad;
+            for (int i = tid; i < NU; i += NT) Q.RU[(size_t)e * NU + i] = s_R[i];
+            if (tid == 0 && Q.status) Q.status[e] = *s_bad;
             __syncthreads();
             continue;
         }
@@ -981,7 +1012,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
 
         // ================================ DUDG = [du, MiRq + MiC du] (schur_primal.m:112-116)
         {
-            double *g_dudg = P.DUDG + (size_t)e * NPV * P.nco;
+            double *g_dudg = Q.DUDG + (size_t)e * NPV * Q.nco;
             for (int i = tid; i < NQ; i += NT) {
                 const int r = i % NPV, c = i / NPV;
                 double v;
@@ -994,7 +1025,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                     for (int s = 0; s < NPV; s++) v += s_MiC[r + NPV * (s + NPV * d)] * s_R[s + NPV * a];
                 }
                 s_dudg[i] = v;
-                if (c < P.nco) g_dudg[i] = v;       // getdqdg = 0: the u rows only
+                if (c < Q.nco) g_dudg[i] = v;       // getdqdg = 0: the u rows only
             }
         }
         __syncthreads();
@@ -1009,7 +1040,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                 Xg[i] = t;
             }
             __syncthreads();
-            double *g_fe = P.FE + (size_t)e * NH;
+            double *g_fe = Q.FE + (size_t)e * NH;
             for (int i = tid; i < NH; i += NT) {
                 const int a = i % NCU, nf = i / NCU, n = nf % NPF, j = nf / NPF;
                 double t = 0.0;
@@ -1036,8 +1067,8 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             constexpr int T = L::TILE;
             constexpr int TMQ = NPV <= 6 ? NPV : (NPV + 1) / 2;
             double *yX = sm + L::y_X, *yXg = sm + L::y_Xg, *yY = sm + L::y_Y;
-            double *g_dd = P.DUDG_DUH + (size_t)e * NPV * NCO * NH;     // [npv, nco, ncu, ndf]
-            double *g_ae = P.AE + (size_t)e * NH * NH;
+            double *g_dd = Q.DUDG_DUH + (size_t)e * NPV * NCO * NH;     // [npv, nco, ncu, ndf]
+            double *g_ae = Q.AE + (size_t)e * NH * NH;
             for (int k0 = 0; k0 < NH; k0 += T) {
                 const int nt = (NH - k0) < T ? (NH - k0) : T;
                 for (int i = tid; i < NU * nt; i += NT) {
@@ -1096,9 +1127,9 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                 __syncthreads();
             }
         };
-        if (P.nco == NC) tiles(std::integral_constant<int, NC>{});
+        if (Q.nco == NC) tiles(std::integral_constant<int, NC>{});
         else tiles(std::integral_constant<int, NCU>{});
-        if (tid == 0 && P.status) P.status[e] = *s_bad;
+        if (tid == 0 && Q.status) Q.status[e] = *s_bad;
         __syncthreads();
     }
     if constexpr (USE_TC) {
@@ -1109,14 +1140,14 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
 }
 
 // ------------------------------------------------------------------ dispatch
-template <class D, bool VISC, bool MIXED>
-static int launch_t(const ElemParams &p, cudaStream_t st, int grid_req) {
+template <class D, bool VISC, bool MIXED, class Arg>
+static int launch_t(const Arg &p, int ne, cudaStream_t st, int grid_req) {
     constexpr int NT = cta_threads<D, VISC, MIXED>();
     using L = PlanSel<D, VISC, MIXED>;
     static_assert(L::TILE >= 1, "tile");
     const size_t smem = L::bytes;
     if (smem > 227 * 1024) return -3;
-    auto kern = elemental_kernel<D, VISC, MIXED, NT>;
+    auto kern = elemental_kernel<D, VISC, MIXED, NT, Arg>;
     cudaError_t err = allow_dynamic_smem((const void *)kern, smem);
     if (err != cudaSuccess) return -10;
     // resident CTAs per SM of this instantiation, once per device
@@ -1129,7 +1160,7 @@ static int launch_t(const ElemParams &p, cudaStream_t st, int grid_req) {
         per_sm_cache[dev < kMaxDevices ? dev : 0].store(per_sm, std::memory_order_relaxed);
     }
     int grid = grid_req > 0 ? grid_req : nsm * per_sm;     // default: one wave of resident CTAs
-    if (grid > p.ne) grid = p.ne;
+    if (grid > ne) grid = ne;
     if (grid < 1) return 0;
     kern<<<grid, NT, smem, st>>>(p);
     err = cudaGetLastError();
@@ -1138,8 +1169,8 @@ static int launch_t(const ElemParams &p, cudaStream_t st, int grid_req) {
 
 template <class D>
 static int launch_v(const ElemParams &p, bool visc, bool mixed, cudaStream_t st, int grid) {
-    if (mixed) return visc ? launch_t<D, true, true>(p, st, grid) : launch_t<D, false, true>(p, st, grid);
-    return visc ? launch_t<D, true, false>(p, st, grid) : launch_t<D, false, false>(p, st, grid);
+    if (mixed) return visc ? launch_t<D, true, true>(p, p.ne, st, grid) : launch_t<D, false, true>(p, p.ne, st, grid);
+    return visc ? launch_t<D, true, false>(p, p.ne, st, grid) : launch_t<D, false, false>(p, p.ne, st, grid);
 }
 
 // The compiled element shapes, keyed by (nd, porder).  Their Gauss point counts are those of
@@ -1177,10 +1208,9 @@ int elemental_check_master(const hdgx_master *m) {
     });
 }
 
-int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const double *dgnodes,
-                     const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
-                     double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed,
-                     int grid, double *QDG, double *RU) {
+static ElemParams fill_params(const hdgx_master *m, const hdgx_app *app, int ne, const double *dgnodes,
+                              const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
+                              double *FE, double *DUDG, double *DUDG_DUH, int *status, double *QDG, double *RU) {
     ElemParams p;
     p.shapvt = m->shapvt; p.shapvg = m->shapvg; p.shapmv = m->shapmv;
     p.shapft = m->shapft; p.shapfg = m->shapfg; p.shapmf = m->shapmf; p.perm = m->perm;
@@ -1204,10 +1234,58 @@ int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const do
     p.QDG = QDG;
     p.RU = RU;
     p.nco = app->getdqdg ? app->nc : app->ncu;
-    const bool visc = p.pc.rinv != 0.0;
+    return p;
+}
+
+static bool is_viscous(const hdgx_app *app) {
+    const double re = app->param[2];
+    return re > 0.0 && isfinite(re);
+}
+
+int elemental_launch(const hdgx_master *m, const hdgx_app *app, int ne, const double *dgnodes,
+                     const int *bf, const double *UDG, const double *UH, const double *SH, double *AE,
+                     double *FE, double *DUDG, double *DUDG_DUH, int *status, cudaStream_t st, bool mixed,
+                     int grid, double *QDG, double *RU) {
+    const ElemParams p = fill_params(m, app, ne, dgnodes, bf, UDG, UH, SH, AE, FE, DUDG, DUDG_DUH, status, QDG, RU);
     if (int rc = elemental_check_master(m)) return rc;   // nothing is launched for a foreign master
     return with_dims(m->nd, m->porder, [&](auto d) -> int {
-        return launch_v<decltype(d)>(p, visc, mixed, st, grid);
+        return launch_v<decltype(d)>(p, is_viscous(app), mixed, st, grid);
+    });
+}
+
+int elemental_shared_max_segments() { return kMaxSeg; }
+
+// One FP64 launch over the buckets' elements (callers have validated every bucket).  The buckets
+// must have one element shape (nd, porder and the master's table sizes) and agree on whether the
+// physics is viscous, which selects the kernel; each keeps its own app (physics constants,
+// boundary data, getdqdg) and arrays.  The master tables are read from bucket 0's master.
+int elemental_launch_shared(int nb, const hdgx_elem_bucket *b, cudaStream_t st, int grid) {
+    if (nb < 1 || nb > kMaxSeg) return -1;
+    const hdgx_master *m0 = b[0].master;
+    const bool visc = is_viscous(b[0].app);
+    for (int k = 1; k < nb; k++) {
+        const hdgx_master *m = b[k].master;
+        if (m->nd != m0->nd || m->porder != m0->porder || m->npv != m0->npv || m->npf != m0->npf ||
+            m->ngv != m0->ngv || m->ngf != m0->ngf)
+            return -2;
+        if (is_viscous(b[k].app) != visc) return -2;
+    }
+    if (int rc = elemental_check_master(m0)) return rc;
+    SegTable t;
+    int n = 0;
+    for (int k = 0; k < nb; k++) {
+        const hdgx_elem_bucket &q = b[k];
+        t.seg[k] = fill_params(m0, q.app, q.ne, q.dgnodes, q.bf, q.UDG, q.UH, q.SH, q.AE, q.FE, q.DUDG, q.DUDG_DUH,
+                               q.status, nullptr, nullptr);
+        t.seg_start[k] = n;
+        n += q.ne;
+    }
+    t.seg_start[nb] = n;
+    t.nseg = nb;
+    if (n == 0) return 0;
+    return with_dims(m0->nd, m0->porder, [&](auto d) -> int {
+        using D = decltype(d);
+        return visc ? launch_t<D, true, false>(t, n, st, grid) : launch_t<D, false, false>(t, n, st, grid);
     });
 }
 

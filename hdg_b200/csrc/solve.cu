@@ -20,6 +20,10 @@
 namespace hdgx {
 
 int elemental_check_master(const hdgx_master *m);
+int combiner_attach(hdgx_combiner *c, uint64_t key);
+void combiner_detach(hdgx_combiner *c, uint64_t key);
+int combiner_key(hdgx_combiner *c, const hdgx_master *m, const hdgx_app *app, cudaStream_t st, uint64_t *key);
+int combiner_submit(hdgx_combiner *c, const hdgx_elem_bucket &b, uint64_t key, cudaStream_t st);
 
 // y = x0 + alpha * d   (the line-search update hdg_solve.m:146-147)
 __global__ void add_scaled_kernel(size_t n, const double *__restrict__ x0, double alpha, const double *__restrict__ d,
@@ -212,9 +216,7 @@ struct DevPool {
 };
 
 double norm2(size_t n, const double *x, double *part, double *out, cudaStream_t st) {
-    int nsm = 0, dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int nsm = sm_count_of(current_device());
     size_t g = (n + 255) / 256;
     if (g > (size_t)nsm * 8) g = (size_t)nsm * 8;
     if (g > 1024) g = 1024;
@@ -235,9 +237,20 @@ cudaMemPool_t device_pool() { return solve_pool(); }
 
 using namespace hdgx;
 
-extern "C" int hdgx_solve(const hdgx_master *m, const hdgx_app *app, const hdgx_mesh *mesh, double *UDG, double *UH,
-                          const double *SH, const hdgx_solve_opts *opts, hdgx_solve_report *rep,
-                          hdgx_stream_t stream) {
+namespace {
+
+// A solve's membership of a combiner.
+struct CombinerLink {
+    hdgx_combiner *c = nullptr;
+    uint64_t key = 0;
+    ~CombinerLink() {
+        if (c) combiner_detach(c, key);
+    }
+};
+
+int solve_impl(const hdgx_master *m, const hdgx_app *app, const hdgx_mesh *mesh, double *UDG, double *UH,
+               const double *SH, const hdgx_solve_opts *opts, hdgx_solve_report *rep, hdgx_combiner *comb,
+               hdgx_stream_t stream) {
     if (!m || !app || !mesh || !UDG || !UH || !SH || !opts) return -1;
     if (!mesh->dgnodes || !mesh->bf || !mesh->elcon || !mesh->t2f || !mesh->rowpts || !mesh->colind) return -1;
     const int ne = mesh->ne, nf = mesh->nf;
@@ -245,7 +258,14 @@ extern "C" int hdgx_solve(const hdgx_master *m, const hdgx_app *app, const hdgx_
     if (app->getdqdg != 1) return -2;    // the native loop keeps q in the local solve (getdqdg = 1)
     if (int rc = hdgx::elemental_check_master(m)) return rc;   // before any set-up or allocation
     if (opts->ordering != 0 && opts->ordering != 1) return -1;
+    if (comb && opts->mixed) return -2;                         // shared launches are FP64
     cudaStream_t st = (cudaStream_t)stream;
+    CombinerLink link;
+    if (comb) {
+        if (int rc = combiner_key(comb, m, app, st, &link.key)) return rc;
+        if (int rc = combiner_attach(comb, link.key)) return rc;
+        link.c = comb;
+    }
     const int npv = m->npv, npf = m->npf, nfe = m->nfe, ncu = app->ncu, nc = app->nc;
     const int ndf = npf * nfe, bs = ncu * npf;
     const long long nnzb = mesh->rowpts[nf];
@@ -305,10 +325,16 @@ extern "C" int hdgx_solve(const hdgx_master *m, const hdgx_app *app, const hdgx_
     auto assemble = [&](double *res) -> int {
         int rc = hdgx_gather_uh(ncu, ndf, ne, mesh->elcon, UH, UHe, stream);
         if (rc) return rc;
-        rc = opts->mixed ? hdgx_elemental_mixed(m, app, ne, mesh->dgnodes, mesh->bf, UDG, UHe, SH, AE, FE, DUDG,
-                                                DUDG_DUH, status, stream)
-                         : hdgx_elemental(m, app, ne, mesh->dgnodes, mesh->bf, UDG, UHe, SH, AE, FE, DUDG, DUDG_DUH,
-                                          status, stream);
+        if (comb) {
+            const hdgx_elem_bucket b = {m, app, ne, mesh->dgnodes, mesh->bf, UDG, UHe, SH, AE, FE, DUDG, DUDG_DUH,
+                                        status, 0};
+            rc = combiner_submit(comb, b, link.key, st);
+        } else {
+            rc = opts->mixed ? hdgx_elemental_mixed(m, app, ne, mesh->dgnodes, mesh->bf, UDG, UHe, SH, AE, FE, DUDG,
+                                                    DUDG_DUH, status, stream)
+                             : hdgx_elemental(m, app, ne, mesh->dgnodes, mesh->bf, UDG, UHe, SH, AE, FE, DUDG,
+                                              DUDG_DUH, status, stream);
+        }
         if (rc) return rc;
         rc = hdgx_globalassembly(&A, &map, ncu, npf, nfe, mesh->elcon, AE, FE, Hg, Rg, stream);
         if (rc) return rc;
@@ -384,4 +410,19 @@ extern "C" int hdgx_solve(const hdgx_master *m, const hdgx_app *app, const hdgx_
     r.ncolors = A.ncolors;
     if (rep) *rep = r;
     return cudaGetLastError() == cudaSuccess ? 0 : -12;
+}
+
+}  // namespace
+
+extern "C" int hdgx_solve(const hdgx_master *m, const hdgx_app *app, const hdgx_mesh *mesh, double *UDG, double *UH,
+                          const double *SH, const hdgx_solve_opts *opts, hdgx_solve_report *rep,
+                          hdgx_stream_t stream) {
+    return solve_impl(m, app, mesh, UDG, UH, SH, opts, rep, nullptr, stream);
+}
+
+extern "C" int hdgx_solve_combined(const hdgx_master *m, const hdgx_app *app, const hdgx_mesh *mesh, double *UDG,
+                                   double *UH, const double *SH, const hdgx_solve_opts *opts, hdgx_solve_report *rep,
+                                   hdgx_combiner *combiner, hdgx_stream_t stream) {
+    if (!combiner) return -1;
+    return solve_impl(m, app, mesh, UDG, UH, SH, opts, rep, combiner, stream);
 }

@@ -92,16 +92,17 @@ def request_mix(seed, count, nmin=8, nmax=24, pmin=1, pmax=4, rate=20.0):
     return reqs
 
 
-def _solve_one(req, ordering, mixed, restart, engine="native"):
+def _solve_one(req, ordering, mixed, restart, engine="native", combiner=None):
     """One request on the current CUDA stream.  engine "native": one hdgx_solve call (the
     Newton loop and its host-side set-up in the library, which runs without the Python
-    interpreter lock, so concurrent requests also overlap on the host); "python": the
+    interpreter lock, so concurrent requests also overlap on the host), with its elemental
+    evaluations batched with the other requests' when a ``combiner`` is given; "python": the
     HDGSolver composition of the same kernels."""
     P = req.problem
     if engine == "native":
         from .solve import hdgx_solve
         U, H, rep = hdgx_solve(P.master, P.mesh, P.app, P.UDG, P.UH, P.SH, tol=req.tol, maxiter=req.maxiter,
-                               restart=restart, ordering=ordering, mixed=mixed)
+                               restart=restart, ordering=ordering, mixed=mixed, combiner=combiner)
         req.UDG, req.UH = U, H
         req.converged, req.iterations = rep["converged"], rep["iterations"]
         req.residuals, req.gmres_iters = list(rep["residuals"]), list(rep["gmres_iters"])
@@ -130,16 +131,22 @@ def latency_stats(reqs, t0):
 
 class Server:
     def __init__(self, slots=8, memory_budget=None, ordering="multicolor", mixed=False, restart=20, engine="native",
-                 max_bypass=4):
+                 max_bypass=4, combine=False, window_us=0):
         """max_bypass: how many later requests may be admitted ahead of a waiting request that
         does not fit yet (a large request waiting for memory does not block small ones behind
-        it, but it is not overtaken more than this many times)."""
+        it, but it is not overtaken more than this many times).  combine: the running requests'
+        elemental evaluations of one degree and physics kind share launches (native engine,
+        FP64; ``solve.Combiner`` with ``window_us``)."""
+        if combine and (engine != "native" or mixed):
+            raise ValueError("shared launches need the native engine in FP64")
         if memory_budget is None:
             free, _ = torch.cuda.mem_get_info()
             memory_budget = int(0.8 * free)
         self.slots, self.budget = slots, memory_budget
         self.ordering, self.mixed, self.restart, self.engine = ordering, mixed, restart, engine
         self.max_bypass = max_bypass
+        self.combine, self.window_us = combine, window_us
+        self.combiner_stats = None
 
     def serve(self, reqs, realtime=True):
         """Run the requests with continuous admission; returns latency statistics."""
@@ -149,6 +156,10 @@ class Server:
         streams = [torch.cuda.Stream() for _ in range(self.slots)]
         free_streams = list(range(self.slots))
         dev = torch.cuda.current_device()
+        combiner = None
+        if self.combine:
+            from .solve import Combiner
+            combiner = Combiner(self.window_us)
         t0 = time.perf_counter()
         threads = []
 
@@ -159,7 +170,7 @@ class Server:
             torch.cuda.set_device(dev)
             try:
                 with torch.cuda.stream(streams[sid]):
-                    _solve_one(req, self.ordering, self.mixed, self.restart, self.engine)
+                    _solve_one(req, self.ordering, self.mixed, self.restart, self.engine, combiner)
                 streams[sid].synchronize()
             except Exception as exc:        # a failed request is reported, not fatal
                 req.error = repr(exc)
@@ -212,6 +223,9 @@ class Server:
             threads.append(th)
         for th in threads:
             th.join()
+        if combiner is not None:
+            self.combiner_stats = combiner.stats()
+            combiner.close()
         return latency_stats(reqs, t0)
 
     def serve_sequential(self, reqs, realtime=True):

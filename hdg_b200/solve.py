@@ -335,11 +335,48 @@ def hdg_solve(master, mesh, app, UDG, UH, SH=None, tol=1e-10, maxiter=16, gmres_
     return dU.numpy(), dH.numpy(), rep
 
 
+class Combiner:
+    """Shared elemental launches of concurrent native solves (``hdgx_combiner`` of the C ABI).
+
+    Solves that pass the same combiner to ``hdgx_solve`` and run at the same time (each on its
+    own thread and CUDA stream) have their assemblies' elemental evaluations batched: every group
+    of equal master tables and one physics kind runs as one ``hdgx_elemental_shared`` launch.
+    ``window_us``: how long the first assembly of a batch waits for the other attached solves
+    (0: it takes what is queued at once)."""
+
+    def __init__(self, window_us=0):
+        _require_cuda()
+        h = ct.c_void_p()
+        check(lib().hdgx_combiner_create(int(window_us), ct.byref(h)), "hdgx_combiner_create")
+        self.handle = h
+        self.window_us = int(window_us)
+
+    def stats(self):
+        b, n, s = ct.c_longlong(), ct.c_longlong(), ct.c_longlong()
+        check(lib().hdgx_combiner_stats(self.handle, ct.byref(b), ct.byref(n), ct.byref(s)), "hdgx_combiner_stats")
+        k, w = ct.c_double(), ct.c_double()
+        check(lib().hdgx_combiner_times(self.handle, ct.byref(k), ct.byref(w)), "hdgx_combiner_times")
+        return {"batches": b.value, "launches": n.value, "submissions": s.value, "key_s": k.value,
+                "submit_s": w.value}
+
+    def close(self):
+        if self.handle:
+            check(lib().hdgx_combiner_destroy(self.handle), "hdgx_combiner_destroy")
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def hdgx_solve(master, mesh, app, UDG, UH, SH=None, tol=1e-10, maxiter=16, gmres_tol=1e-10, restart=20,
-               ordering="mdf", mixed=False, gmres_maxit=1000, stream=None):
+               ordering="mdf", mixed=False, gmres_maxit=1000, stream=None, combiner=None):
     """kernel/hdg_solve.m as ONE native call (``hdgx_solve`` of the C ABI): the Newton loop,
     the elimination order and the assembly map are built inside the library.  Returns
-    (UDG, UH, report dict) as host arrays; the inputs are not modified."""
+    (UDG, UH, report dict) as host arrays; the inputs are not modified.  ``combiner``: a
+    ``Combiner`` shared with concurrent solves (``hdgx_solve_combined``, FP64 only)."""
     from ._lib import HDGX_SOLVE_MAXIT, HdgxMesh, HdgxSolveOpts, HdgxSolveReport
     _require_cuda()
     if maxiter > HDGX_SOLVE_MAXIT:
@@ -359,8 +396,12 @@ def hdgx_solve(master, mesh, app, UDG, UH, SH=None, tol=1e-10, maxiter=16, gmres
     dH = DArray.from_numpy(UH)
     dS = DArray.from_numpy(np.zeros_like(UDG) if SH is None else SH)
     rep = HdgxSolveReport()
-    rc = lib().hdgx_solve(ct.byref(dm.c), ct.byref(appc), ct.byref(cm), dU.ptr, dH.ptr, dS.ptr, ct.byref(opts),
-                          ct.byref(rep), _stream_ptr(stream))
+    if combiner is None:
+        rc = lib().hdgx_solve(ct.byref(dm.c), ct.byref(appc), ct.byref(cm), dU.ptr, dH.ptr, dS.ptr, ct.byref(opts),
+                              ct.byref(rep), _stream_ptr(stream))
+    else:
+        rc = lib().hdgx_solve_combined(ct.byref(dm.c), ct.byref(appc), ct.byref(cm), dU.ptr, dH.ptr, dS.ptr,
+                                       ct.byref(opts), ct.byref(rep), combiner.handle, _stream_ptr(stream))
     check(rc, "hdgx_solve")
     n = rep.iterations
     report = dict(iterations=n, converged=bool(rep.converged), levels=rep.ncolors,

@@ -45,6 +45,7 @@ extern "C" {
 #endif
 
 typedef struct CUstream_st *hdgx_stream_t;   /* a cudaStream_t; NULL = legacy default stream */
+typedef struct hdgx_combiner hdgx_combiner;  /* shared elemental launches of concurrent solves */
 
 /* Master element tables (master/mkmaster.m + util/preprocess.m:23-55), DEVICE pointers. */
 typedef struct {
@@ -170,6 +171,20 @@ typedef struct {
 } hdgx_elem_bucket;
 
 int hdgx_elemental_buckets(int nb, const hdgx_elem_bucket *buckets, int mixed, hdgx_stream_t stream);
+
+/* One FP64 elemental launch over the elements of several buckets of ONE element shape (the same
+ * nd and porder, masters of the same table sizes; the master tables are read from buckets[0]) and
+ * one kind of physics (all viscous, Re finite, or all inviscid): each bucket keeps its own app
+ * (constants, boundary data, getdqdg), arrays and status, and its results are bitwise those of
+ * hdgx_elemental on that bucket alone.  For callers that evaluate many small independent meshes
+ * at once (a serving loop), where one launch fills the GPU that one bucket alone would not.
+ * At most hdgx_elemental_shared_max() buckets (-5 beyond); -2 when the buckets' shapes or physics
+ * kinds differ; the buckets' `grid` fields are ignored, `grid` = CTAs of the launch (0: one wave
+ * of resident CTAs).  The bucket table travels as the kernel's parameter: nothing is allocated or
+ * copied, and the call can be captured in a CUDA graph.  No counterpart in the reference, which
+ * assembles one mesh per call (kernel/hdg_assemble.m). */
+int hdgx_elemental_shared(int nb, const hdgx_elem_bucket *buckets, int grid, hdgx_stream_t stream);
+int hdgx_elemental_shared_max(void);
 
 /* Batched u-only Schur complement (kernel/schur_u.c): BD[npv,ncu,npv,nc,ne] (only the
  * first ncu component columns are read), F, GK[ncu,ndf,npv,nc,ne], H, Ru, Rh ->
@@ -378,6 +393,28 @@ typedef struct {
  * calls.  The call synchronises the stream (it reads residual norms on the host). */
 int hdgx_solve(const hdgx_master *master, const hdgx_app *app, const hdgx_mesh *mesh, double *UDG, double *UH,
                const double *SH, const hdgx_solve_opts *opts, hdgx_solve_report *report, hdgx_stream_t stream);
+
+/* Shared elemental launches across concurrent solves (serving).  A combiner collects the assemblies
+ * of the hdgx_solve_combined calls that run at the same time (each on its own host thread and
+ * stream) and evaluates each group of equal master tables and one physics kind (viscous or not)
+ * as one hdgx_elemental_shared launch on one of the combiner's streams; every solve's results are bitwise
+ * those of hdgx_solve.  The first submission of a batch waits until every attached solve of its
+ * group has submitted or window_us microseconds have passed (0: it takes what is queued at once).  One
+ * combiner serves one device (the current device at creation; -2 for solves on another).
+ * hdgx_solve_combined: arguments of hdgx_solve plus the combiner; FP64 only (opts->mixed = 1
+ * returns -2); the call reads the master tables once to key its group.  Destroy only when no
+ * solve is attached (-1 otherwise).  No counterpart in the reference (kernel/hdg_solve.m solves one
+ * problem per call). */
+int hdgx_combiner_create(int window_us, hdgx_combiner **out);
+int hdgx_combiner_destroy(hdgx_combiner *combiner);
+int hdgx_combiner_stats(const hdgx_combiner *combiner, long long *batches, long long *launches,
+                        long long *submissions);
+/* Host seconds all solves spent keying their group (reading the master tables) and in submissions
+ * (queueing, waiting for a batch, launching). */
+int hdgx_combiner_times(const hdgx_combiner *combiner, double *key_s, double *submit_s);
+int hdgx_solve_combined(const hdgx_master *master, const hdgx_app *app, const hdgx_mesh *mesh, double *UDG,
+                        double *UH, const double *SH, const hdgx_solve_opts *opts, hdgx_solve_report *report,
+                        hdgx_combiner *combiner, hdgx_stream_t stream);
 
 /* ------------------------------------------------- dense face-block path (app.denseblock = 1) */
 

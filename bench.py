@@ -508,6 +508,7 @@ def main():
             line["buckets"] = buckets_mixed_degree(torch, use_mixed)
         if not args.no_serve and ws == 1:
             line["serve"] = serve_mix(torch)
+            line["serve"]["shared_launch"] = shared_launch(torch)
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.barrier()
@@ -591,6 +592,14 @@ def serve_mix(torch, count=16, slots=8, ordering="mdf"):
     c5_seq = Server(slots=1, ordering=ordering).serve_sequential(request_mix(21, count, **c5kw))
     c5_conc_reqs = request_mix(21, count, **c5kw)
     c5_conc = Server(slots=slots, ordering=ordering).serve(c5_conc_reqs)
+    # the same stream with the running requests' same-degree, same-physics assemblies batched into
+    # shared launches (hdgx_solve_combined, 1 ms batching window)
+    comb_srv = Server(slots=slots, ordering=ordering, combine=True, window_us=1000)
+    c5_comb_reqs = request_mix(21, count, **c5kw)
+    c5_comb = comb_srv.serve(c5_comb_reqs)
+    c5_comb["combiner"] = comb_srv.combiner_stats
+    c5_comb["identical_to_uncombined"] = all(np.array_equal(a.UDG, b.UDG) and np.array_equal(a.UH, b.UH)
+                                             for a, b in zip(c5_conc_reqs, c5_comb_reqs))
     torch.cuda.empty_cache()
     return {"requests": count, "slots": slots, "ordering": ordering, "newton_tol": 1e-10,
             "mix": "2D n x n x 2, n 8-20, p 1-4, M 0.3-0.8, half Euler / half NS Re 200-2000, Poisson 20/s (seed 11)",
@@ -602,8 +611,38 @@ def serve_mix(torch, count=16, slots=8, ordering="mdf"):
             "c5_subset": {"mix": f"C5 distribution truncated to n 24-40: {count} requests, 2D n x n x 2, p 1-4, "
                                  "M 0.3-0.8, half Euler / half NS Re 200-2000, Poisson 20/s (seed 21)",
                           "elements": int(sum(r.problem.mesh.ne for r in c5_conc_reqs)),
-                          "concurrent": c5_conc, "sequential": c5_seq,
+                          "concurrent": c5_conc, "sequential": c5_seq, "concurrent_shared_launches": c5_comb,
                           "speedup_solves_per_s": c5_conc["solves_per_s"] / c5_seq["solves_per_s"]}}
+
+
+def shared_launch(torch, count=24, n=6, p=3, steps=20):
+    """Many small independent problems of one degree (24 NS requests on 6 x 6 x 2 triangles at
+    p = 3, each with its own Re, Mach and state): one elemental evaluation of all of them per step,
+    as ONE segmented launch (hdgx_elemental_shared) against one launch per problem on one stream.
+    Outputs are bitwise equal (tests/test_shared_gpu.py)."""
+    from hdg_b200.batch import SharedLaunch
+    from hdg_b200.serve import request_mix
+    rs = request_mix(31, 2 * count, nmin=n, nmax=n, pmin=p, pmax=p)
+    sl = SharedLaunch([r.problem for r in rs if r.rid % 2 == 1][:count])
+    st = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms_shared = timed(lambda: sl.run(stream=st))
+    ms_each = timed(lambda: sl.run_each(stream=st))
+    return {"problems": len(sl.items), "elements": sl.ne, "workload": f"{count} NS problems, {n}x{n}x2 triangles, p={p}",
+            "shared_ms": ms_shared, "per_problem_ms": ms_each, "speedup": ms_each / ms_shared,
+            "shared_elements_per_s": sl.ne / (ms_shared * 1e-3)}
 
 
 def newton_step(P, torch, args):

@@ -43,6 +43,7 @@ struct ElemParams {
     double *QDG;               // non-NULL: getq mode (kernel/getq.m), the element stops after inv(M)
     int nco;                   // components stored in DUDG / DUDG_DUH: nc, or ncu when app.getdqdg = 0
     double *RU;                // non-NULL: residual mode (kernel/cuda_residual.m), Ru at q = getq(u, uh)
+    double *ws;                // global workspace of plans beyond shared memory (set by the launcher)
 };
 
 // One launch over the same-shape elements of several independent element sets (e.g. of several
@@ -174,7 +175,7 @@ struct Plan {
     static constexpr int d_b0 = d_diag + D::NU;                         // [NU] first right-hand side
     static constexpr int d_invsep = d_b0 + D::NU;                       // [NU*NU] FP32-accurate SD^-1 (MIXED)
     static constexpr int d_mbar = d_invsep + ((MIXED && !INV_ALIAS) ? D::NU * D::NU : 0);   // tensor-core mbarrier
-    static constexpr int n_doubles = d_mbar + (MIXED ? 4 : 0);                    // two mbarriers (16-byte slot each)
+    static constexpr int n_doubles_core = d_mbar + (MIXED ? 4 : 0);               // two mbarriers (16-byte slot each)
     static constexpr int d_inv = INV_ALIAS ? x_start + (SD_ALIAS ? D::NU * D::NU : 0) : d_invsep;
     // Tensor-core Schur product of the mixed form, X = SD^-1 [B Mi E - F] (tcgen05, 3xTF32): the
     // operands, SD^-1 as A (M = 128 rows of which NU are real, K = NU padded to the MMA step) and
@@ -191,9 +192,7 @@ struct Plan {
     static constexpr TcPlace TCP = tc_place(MIXED, x_start, inv_lo, inv_hi, x_end, TC_ADBL, TC_KC, TC_NP);
     static constexpr int TC_PL = TCP.pl, TC_NB = TCP.nb, TC_NBUF = TCP.nbuf, tc_a = TCP.a, tc_b = TCP.b;
     static constexpr int TC_BSTRIDE = al16(2 * (TC_NB / 8) * TC_KC * 128 / 8);   // doubles between B tiles
-    static constexpr bool TC = TC_PL != 0 && tc_a * 8 + 16 * TC_KC * 128 <= (int)(sizeof(double) * n_doubles) &&
-                               TC_NP <= 256 && D::NU <= 64;
-    // integers after the doubles
+    // integers (after the doubles in shared memory)
     static constexpr int i_perm = 0;                      // [NPF, NFE] 0-based
     static constexpr int i_invp = D::NPF * D::NFE;        // [NPV, NFE] face-local index or -1
     static constexpr int i_piv = i_invp + D::NPV * D::NFE;
@@ -205,7 +204,19 @@ struct Plan {
     static constexpr int i_bad = i_bf + D::NFE;
     static constexpr int i_tmem = i_bad + 1;              // TMEM address of the tensor-core accumulator
     static constexpr int n_ints = i_tmem + 1;
-    static constexpr size_t bytes = sizeof(double) * n_doubles + sizeof(int) * n_ints;
+    // Plans beyond a CTA's shared memory (3D p = 3: 520 KB for 100 unknowns and 201 right-hand
+    // sides) keep every double array in a per-CTA slice of a global workspace, read and written
+    // through L1 (one CTA per SM, the shared-memory carveout at its minimum), with the integers in
+    // shared memory; the local system is then eliminated in memory with partial pivoting
+    // (block_gauss_jordan), which leaves the solution rows in pivot order: d_perm re-orders them.
+    static constexpr bool WS = sizeof(double) * n_doubles_core + sizeof(int) * n_ints > 227 * 1024;
+    static constexpr int d_perm = n_doubles_core;                          // WS: [NU, 1 + NH]
+    static constexpr int n_doubles = n_doubles_core + (WS ? D::NU * (1 + D::NH) : 0);
+    static constexpr int ws_stride = al16(n_doubles);                       // doubles per CTA slice
+    static constexpr bool TC = !WS && TC_PL != 0 && tc_a * 8 + 16 * TC_KC * 128 <= (int)(sizeof(double) * n_doubles) &&
+                               TC_NP <= 256 && D::NU <= 64;
+    static constexpr size_t bytes = sizeof(double) * n_doubles + sizeof(int) * n_ints;   // the whole plan
+    static constexpr size_t smem_bytes = WS ? sizeof(int) * n_ints : bytes;             // of it in shared memory
 };
 
 // Resident elements per SM: the kernel is latency-bound (barrier-separated phases, a 40-step
@@ -220,7 +231,8 @@ constexpr int blocks_for(size_t bytes) {
 }
 template <class D, bool VISC, bool MIXED>
 using PlanSel = Plan<D, VISC, MIXED,
-                     (blocks_for(Plan<D, VISC, MIXED, false>::bytes) <= blocks_for(Plan<D, VISC, MIXED, true>::bytes))>;
+                     (!Plan<D, VISC, MIXED, false>::WS &&
+                      blocks_for(Plan<D, VISC, MIXED, false>::bytes) <= blocks_for(Plan<D, VISC, MIXED, true>::bytes))>;
 template <class D, bool VISC, bool MIXED>
 constexpr int min_blocks() { return blocks_for(PlanSel<D, VISC, MIXED>::bytes); }
 template <class D, bool VISC, bool MIXED>
@@ -247,11 +259,13 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     constexpr int NSEED = VISC ? NC : NCU;   // inviscid flux does not depend on q
     constexpr int NCG = VISC ? NC : NCU;     // components dRh/dudg couples (q-part is 0 for Euler)
     extern __shared__ __align__(16) double sm[];
-    int *si = reinterpret_cast<int *>(sm + L::n_doubles);
+    // the doubles of the plan: shared memory, or this CTA's slice of the global workspace
+    double *wk = L::WS ? P.ws + (size_t)blockIdx.x * L::ws_stride : sm;
+    int *si = L::WS ? reinterpret_cast<int *>(sm) : reinterpret_cast<int *>(sm + L::n_doubles);
     const int tid = threadIdx.x;
 
-    const double *t_vt = L::TABLES ? sm + L::t_vt : P.shapvt, *t_vg = L::TABLES ? sm + L::t_vg : P.shapvg;
-    double *t_ft = sm + L::t_ft, *t_fg = sm + L::t_fg;
+    const double *t_vt = L::TABLES ? wk + L::t_vt : P.shapvt, *t_vg = L::TABLES ? wk + L::t_vg : P.shapvg;
+    double *t_ft = wk + L::t_ft, *t_fg = wk + L::t_fg;
     const double *__restrict__ t_mv = P.shapmv;   // geometry tables: read once per element from L1
     const double *__restrict__ t_mf = P.shapmf;
     int *perm = si + L::i_perm, *invp = si + L::i_invp;
@@ -259,8 +273,8 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     // ---- master tables, once per CTA
     if constexpr (L::TABLES) {
         for (int i = tid; i < NGV * NPV * (ND + 1); i += NT) {
-            sm[L::t_vt + i] = P.shapvt[i];
-            sm[L::t_vg + i] = P.shapvg[i];
+            wk[L::t_vt + i] = P.shapvt[i];
+            wk[L::t_vg + i] = P.shapvg[i];
         }
     }
     for (int i = tid; i < NGF * NPF; i += NT) {
@@ -278,7 +292,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     // are bound by the latency of their elimination chain: the tensor-core Schur product is used
     // where the plan runs one CTA per SM anyway (3D p = 2).
     constexpr bool USE_TC = L::TC && (min_blocks<D, VISC, MIXED>() == 1 || kTcMultiCta);
-    uint64_t *s_mbar = reinterpret_cast<uint64_t *>(sm + L::d_mbar);
+    uint64_t *s_mbar = reinterpret_cast<uint64_t *>(wk + L::d_mbar);
     uint32_t tmem = 0, tc_phases = 0;          // bit b: the phase parity mbarrier b waits for next
     if constexpr (USE_TC) {
         if (tid < 32) tc::tmem_alloc<TC_COLS>(reinterpret_cast<uint32_t *>(si + L::i_tmem));
@@ -295,21 +309,21 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         tmem = *reinterpret_cast<const uint32_t *>(si + L::i_tmem);
     }
 
-    double *s_dg = sm + L::p_dg, *s_udg = sm + L::p_udg, *s_uh = sm + L::p_uh;
-    double *s_SD = sm + L::p_SD, *s_R = sm + L::p_R;
-    double *s_MiC = sm + L::p_MiC, *s_MiE = sm + L::p_MiE, *s_MiRq = sm + L::p_MiRq;
-    double *s_Gp = sm + L::p_Gp, *s_Hp = sm + L::p_Hp, *s_Rh = sm + L::p_Rh, *s_M = sm + L::p_M;
-    double *s_dudg = sm + L::p_dudg, *s_jv = sm + L::p_jv;
-    double *x_Xx = sm + L::x_Xx, *x_jac = sm + L::x_jac, *x_nl = sm + L::x_nl, *x_jf = sm + L::x_jf;
-    double *x_ug = sm + L::x_ug, *x_fu = sm + L::x_fu, *x_fuh = sm + L::x_fuh;
-    double *x_wrk = sm + L::x_wrk, *x_wrl = sm + L::x_wrl, *x_FH = sm + L::x_FH, *x_BH = sm + L::x_BH;
-    double *x_FHu = sm + L::x_FHu, *x_FHh = sm + L::x_FHh;
-    double *x_Zc = sm + L::x_Zc, *x_Ze = sm + L::x_Ze, *x_Zr = sm + L::x_Zr;
-    double *x_ZFc = sm + L::x_ZFc, *x_ZFe = sm + L::x_ZFe, *x_ZFr = sm + L::x_ZFr;
+    double *s_dg = wk + L::p_dg, *s_udg = wk + L::p_udg, *s_uh = wk + L::p_uh;
+    double *s_SD = wk + L::p_SD, *s_R = wk + L::p_R;
+    double *s_MiC = wk + L::p_MiC, *s_MiE = wk + L::p_MiE, *s_MiRq = wk + L::p_MiRq;
+    double *s_Gp = wk + L::p_Gp, *s_Hp = wk + L::p_Hp, *s_Rh = wk + L::p_Rh, *s_M = wk + L::p_M;
+    double *s_dudg = wk + L::p_dudg, *s_jv = wk + L::p_jv;
+    double *x_Xx = wk + L::x_Xx, *x_jac = wk + L::x_jac, *x_nl = wk + L::x_nl, *x_jf = wk + L::x_jf;
+    double *x_ug = wk + L::x_ug, *x_fu = wk + L::x_fu, *x_fuh = wk + L::x_fuh;
+    double *x_wrk = wk + L::x_wrk, *x_wrl = wk + L::x_wrl, *x_FH = wk + L::x_FH, *x_BH = wk + L::x_BH;
+    double *x_FHu = wk + L::x_FHu, *x_FHh = wk + L::x_FHh;
+    double *x_Zc = wk + L::x_Zc, *x_Ze = wk + L::x_Ze, *x_Zr = wk + L::x_Zr;
+    double *x_ZFc = wk + L::x_ZFc, *x_ZFe = wk + L::x_ZFe, *x_ZFr = wk + L::x_ZFr;
     int *s_piv = si + L::i_piv, *s_pivM = si + L::i_pivM, *s_bf = si + L::i_bf, *s_bad = si + L::i_bad;
     int *s_rowused = si + L::i_rowused, *s_rowvar = si + L::i_rowvar, *s_gslot = si + L::i_gslot;
-    unsigned long long *s_slot = reinterpret_cast<unsigned long long *>(sm + L::d_slots);
-    double *s_pcol = sm + L::d_pcol, *s_diag = sm + L::d_diag;
+    unsigned long long *s_slot = reinterpret_cast<unsigned long long *>(wk + L::d_slots);
+    double *s_pcol = wk + L::d_pcol, *s_diag = wk + L::d_diag;
 
     int seg = 0;                                 // segmented launches: the segment of element eg
     const int ne_launch = launch_ne(A);
@@ -831,7 +845,15 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             int bad_before = *s_bad;
             bool tc_go = false;          // the unpivoted mixed solve passed its check: Schur product next
             __syncthreads();
-            if (force_piv) {
+            if constexpr (L::WS) {
+                // the system in memory: Gauss-Jordan with partial pivoting, then the solution rows
+                // (row s_piv[k] holds unknown k) into natural order
+                block_gauss_jordan<NT, true>(s_SD, NU, s_R, NU, NU, 1 + NH, s_piv, s_rowused, s_slot, s_bad);
+                double *s_perm = wk + L::d_perm;
+                for (int t = tid; t < NU * (1 + NH); t += NT) s_perm[t] = s_R[s_piv[t % NU] + NU * (t / NU)];
+                __syncthreads();
+                for (int t = tid; t < NU * (1 + NH); t += NT) s_R[t] = s_perm[t];
+            } else if (force_piv) {
                 gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
             } else {
             // Unpivoted elimination with the density unknowns last (in natural order interior
@@ -839,14 +861,14 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             // the density), accepted when the backward error of the first column,
             // |b0 - SD x0| / (|SD| |x0| + |b0|) (infinity norms), is below 1e-13; otherwise the
             // element is redone with partial pivoting in FP64.
-            double *s_b0 = sm + L::d_b0;
+            double *s_b0 = wk + L::d_b0;
             for (int i = tid; i < NU; i += NT) s_b0[i] = s_R[i];
             __syncthreads();
             if constexpr (MIXED) {
                 // FP32 elimination of [SD | R | I] (with the tensor-core Schur product: of
                 // [SD | r0 | I] only, the other right-hand sides are multiplied by SD^-1 below),
                 // then the residual column refined in FP64 against the FP64 SD with the FP32 inverse
-                double *s_inv = sm + L::d_inv;
+                double *s_inv = wk + L::d_inv;
                 gj_regs_nopiv_t<float, NU, USE_TC ? 1 : 1 + NH, NU, true, NT, 8, NPV>(
                     s_SD, s_R, s_inv, reinterpret_cast<float *>(s_pcol), s_bad);
                 double *s_res = s_pcol;                    // free after the elimination
@@ -934,9 +956,9 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                 if (tc_go) {
                     constexpr int KP = L::TC_KP, KC = L::TC_KC, GR = 8 * L::TC_G, NP = L::TC_NP, NB = L::TC_NB;
                     constexpr int AH = L::TC_G * KC * 128, BH = (NB / 8) * KC * 128;   // bytes of one hi / lo half
-                    const double *s_inv = sm + L::d_inv;
-                    unsigned char *tA = reinterpret_cast<unsigned char *>(sm + L::tc_a);
-                    unsigned char *tB = reinterpret_cast<unsigned char *>(sm + L::tc_b);
+                    const double *s_inv = wk + L::d_inv;
+                    unsigned char *tA = reinterpret_cast<unsigned char *>(wk + L::tc_a);
+                    unsigned char *tB = reinterpret_cast<unsigned char *>(wk + L::tc_b);
                     for (int i = tid; i < GR * KP; i += NT) {
                         const int r = i % GR, k = i / GR;
                         float h = 0.f, l = 0.f;
@@ -1031,7 +1053,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
         __syncthreads();
         // FE = Rh - GK DUDG (schur_primal.m:143-144), GK applied at the face Gauss points
         {
-            double *Xg = sm + L::y_Xg;
+            double *Xg = wk + L::y_Xg;
             for (int i = tid; i < NGT * NCG; i += NT) {
                 const int gg = i % NGT, c = i / NGT, g = gg % NGF, j = gg / NGF;
                 double t = 0.0;
@@ -1066,7 +1088,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             constexpr int NCO = decltype(nco_c)::value;
             constexpr int T = L::TILE;
             constexpr int TMQ = NPV <= 6 ? NPV : (NPV + 1) / 2;
-            double *yX = sm + L::y_X, *yXg = sm + L::y_Xg, *yY = sm + L::y_Y;
+            double *yX = wk + L::y_X, *yXg = wk + L::y_Xg, *yY = wk + L::y_Y;
             double *g_dd = Q.DUDG_DUH + (size_t)e * NPV * NCO * NH;     // [npv, nco, ncu, ndf]
             double *g_ae = Q.AE + (size_t)e * NH * NH;
             for (int k0 = 0; k0 < NH; k0 += T) {
@@ -1140,12 +1162,15 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
 }
 
 // ------------------------------------------------------------------ dispatch
+static ElemParams &base_of(ElemParams &a) { return a; }
+static ElemParams &base_of(SegTable &a) { return a.seg[0]; }
+
 template <class D, bool VISC, bool MIXED, class Arg>
 static int launch_t(const Arg &p, int ne, cudaStream_t st, int grid_req) {
     constexpr int NT = cta_threads<D, VISC, MIXED>();
     using L = PlanSel<D, VISC, MIXED>;
     static_assert(L::TILE >= 1, "tile");
-    const size_t smem = L::bytes;
+    const size_t smem = L::smem_bytes;
     if (smem > 227 * 1024) return -3;
     auto kern = elemental_kernel<D, VISC, MIXED, NT, Arg>;
     cudaError_t err = allow_dynamic_smem((const void *)kern, smem);
@@ -1155,22 +1180,45 @@ static int launch_t(const Arg &p, int ne, cudaStream_t st, int grid_req) {
     const int dev = current_device(), nsm = sm_count_of(dev);
     int per_sm = per_sm_cache[dev < kMaxDevices ? dev : 0].load(std::memory_order_relaxed);
     if (per_sm < 1) {
+        // a plan in the global workspace wants the largest L1 (the smallest shared-memory carveout)
+        if (L::WS && cudaFuncSetAttribute((const void *)kern, cudaFuncAttributePreferredSharedMemoryCarveout, 0) !=
+                         cudaSuccess)
+            return -10;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem) != cudaSuccess) per_sm = 0;
         if (per_sm < 1) return -11;
+        if (L::WS) per_sm = 1;                   // one CTA per SM: its slice stays in L1 / L2
         per_sm_cache[dev < kMaxDevices ? dev : 0].store(per_sm, std::memory_order_relaxed);
     }
     int grid = grid_req > 0 ? grid_req : nsm * per_sm;     // default: one wave of resident CTAs
     if (grid > ne) grid = ne;
     if (grid < 1) return 0;
-    kern<<<grid, NT, smem, st>>>(p);
-    err = cudaGetLastError();
+    if constexpr (L::WS) {
+        // the CTAs' workspace slices, from the stream-ordered allocator (freed behind the launch)
+        Arg q = p;
+        double *ws = nullptr;
+        if (cudaMallocAsync((void **)&ws, sizeof(double) * L::ws_stride * (size_t)grid, st) != cudaSuccess)
+            return -13;
+        base_of(q).ws = ws;
+        kern<<<grid, NT, smem, st>>>(q);
+        err = cudaGetLastError();
+        if (cudaFreeAsync(ws, st) != cudaSuccess && err == cudaSuccess) return -12;
+    } else {
+        kern<<<grid, NT, smem, st>>>(p);
+        err = cudaGetLastError();
+    }
     return err == cudaSuccess ? 0 : -12;
 }
 
 template <class D>
 static int launch_v(const ElemParams &p, bool visc, bool mixed, cudaStream_t st, int grid) {
-    if (mixed) return visc ? launch_t<D, true, true>(p, p.ne, st, grid) : launch_t<D, false, true>(p, p.ne, st, grid);
-    return visc ? launch_t<D, true, false>(p, p.ne, st, grid) : launch_t<D, false, false>(p, p.ne, st, grid);
+    if constexpr (PlanSel<D, true, false>::WS || PlanSel<D, false, false>::WS) {
+        // plans in the global workspace are built in FP64 only: the mixed form runs the FP64 kernel
+        return visc ? launch_t<D, true, false>(p, p.ne, st, grid) : launch_t<D, false, false>(p, p.ne, st, grid);
+    } else {
+        if (mixed)
+            return visc ? launch_t<D, true, true>(p, p.ne, st, grid) : launch_t<D, false, true>(p, p.ne, st, grid);
+        return visc ? launch_t<D, true, false>(p, p.ne, st, grid) : launch_t<D, false, false>(p, p.ne, st, grid);
+    }
 }
 
 // The compiled element shapes, keyed by (nd, porder).  Their Gauss point counts are those of
@@ -1189,6 +1237,7 @@ static int with_dims(int nd, int po, F &&f) {
         switch (po) {
             case 1: return f(Dims<3, 4, 3, 4, 3>{});
             case 2: return f(Dims<3, 10, 6, 11, 6>{});
+            case 3: return f(Dims<3, 20, 10, 24, 12>{});
         }
     }
     return -3;
@@ -1234,6 +1283,7 @@ static ElemParams fill_params(const hdgx_master *m, const hdgx_app *app, int ne,
     p.QDG = QDG;
     p.RU = RU;
     p.nco = app->getdqdg ? app->nc : app->ncu;
+    p.ws = nullptr;
     return p;
 }
 

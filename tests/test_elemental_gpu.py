@@ -24,6 +24,7 @@ CASES = [
     ("c2", dict(n=3, porder=4)),
     ("c4", dict(n=2, porder=1)),
     ("c4", dict(n=2, porder=2)),
+    ("c4", dict(n=2, porder=3)),     # 100 unknowns, 201 right-hand sides: the global-workspace plan
 ]
 
 
@@ -165,3 +166,23 @@ def test_host_array_entry_point_accepts_pageable_memory():
     assert np.all(st == 0)
     for k, o in zip(("AE", "FE", "DUDG", "DUDG_DUH"), outs):
         assert np.array_equal(o, getattr(dev, k).t.cpu().numpy()), k
+
+
+@pytest.mark.gpu
+def test_viscous_tetrahedra_p3_match_oracle(oracle):
+    """3D Navier-Stokes at p = 3 (the workspace plan with the viscous terms), Re = 100."""
+    from hdg_b200.app import make_app
+    from hdg_b200.elemental import hdg_elemental
+    P = configs.c4(n=2, porder=3)
+    P.app = make_app(3, re=100.0, minf=0.4, tau=2.0)
+    m, a = P.master, P.app
+    ref = oracle.hdg_elemental(m, a, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), P.SH)
+    assert ref["nbad"] == 0
+    out = hdg_elemental(m, a, P.mesh.dgnodes, P.mesh.bf, P.UDG, P.uh_elem(), P.SH)
+    assert int(out.status.numpy().max()) == 0
+    for k in ("AE", "FE", "DUDG_DUH"):
+        err = relerr(getattr(out, k).numpy(), ref[k])
+        assert err < TOL, f"{k} relerr {err:.3e}"
+    err = relerr(out.DUDG.numpy(), ref["DUDG"])
+    bound = max(TOL, 10.0 * ulp_sensitivity(oracle, P))
+    assert err < bound, f"DUDG relerr {err:.3e} > {bound:.3e}"

@@ -65,7 +65,7 @@ def test_foreign_quadrature_is_refused_by_buckets_and_solve():
                         ct.byref(rep), None) == -3
 
 
-@pytest.mark.parametrize("nd,porder,pgauss", [(2, 5, 8), (3, 3, 6)])
+@pytest.mark.parametrize("nd,porder,pgauss", [(2, 5, 8), (3, 4, 6)])
 def test_uncompiled_degree_is_refused(nd, porder, pgauss):
     from hdg_b200._lib import lib
     m = hm.mkmaster(nd, porder, pgauss=pgauss)

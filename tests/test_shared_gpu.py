@@ -68,6 +68,18 @@ def test_shared_launch_tetrahedra():
     _check_shared(SharedLaunch(probs))
 
 
+def test_shared_launch_tetrahedra_p3():
+    """Segments on the global-workspace plan (3D p = 3), Euler and NS."""
+    from hdg_b200 import configs
+    from hdg_b200.app import make_app
+    from hdg_b200.batch import SharedLaunch
+    for re in (np.inf, 100.0):
+        probs = [configs.c4(seed=s, n=1, porder=3) for s in (0, 1, 2)]
+        for k, P in enumerate(probs):
+            P.app = make_app(3, re=re, minf=0.3 + 0.1 * k, tau=2.0)
+        _check_shared(SharedLaunch(probs))
+
+
 def test_shared_launch_many_segments_and_empty_one():
     """The most segments one launch takes, one of them with no elements."""
     from hdg_b200._lib import lib

@@ -206,17 +206,24 @@ struct Plan {
     static constexpr int n_ints = i_tmem + 1;
     // Plans beyond a CTA's shared memory (3D p = 3: 520 KB for 100 unknowns and 201 right-hand
     // sides) keep every double array in a per-CTA slice of a global workspace, read and written
-    // through L1 (one CTA per SM, the shared-memory carveout at its minimum), with the integers in
-    // shared memory; the local system is then eliminated in memory with partial pivoting
-    // (block_gauss_jordan), which leaves the solution rows in pivot order: d_perm re-orders them.
+    // through L1 and L2 (one CTA per SM), with the integers in shared memory; the local system is
+    // then LU-factored and solved in shared memory (below).
     static constexpr bool WS = sizeof(double) * n_doubles_core + sizeof(int) * n_ints > 227 * 1024;
-    static constexpr int d_perm = n_doubles_core;                          // WS: [NU, 1 + NH]
-    static constexpr int n_doubles = n_doubles_core + (WS ? D::NU * (1 + D::NH) : 0);
+    static constexpr int n_doubles = n_doubles_core;
     static constexpr int ws_stride = al16(n_doubles);                       // doubles per CTA slice
     static constexpr bool TC = !WS && TC_PL != 0 && tc_a * 8 + 16 * TC_KC * 128 <= (int)(sizeof(double) * n_doubles) &&
                                TC_NP <= 256 && D::NU <= 64;
     static constexpr size_t bytes = sizeof(double) * n_doubles + sizeof(int) * n_ints;   // the whole plan
-    static constexpr size_t smem_bytes = WS ? sizeof(int) * n_ints : bytes;             // of it in shared memory
+    // WS: the local system is LU-factored in shared memory (the factors of SD, NU x NU, after the
+    // integers) and its right-hand sides solved in LU_NCH chunks of LU_CH columns (leading
+    // dimension NU + 1 against bank conflicts)
+    static constexpr int lu_off = al16((n_ints * (int)sizeof(int) + 7) / 8);         // doubles
+    static constexpr int LU_CHMAX = (227 * 1024 / 8 - lu_off - D::NU * D::NU) / (D::NU + 1);
+    static constexpr int LU_NCH = (1 + D::NH + LU_CHMAX - 1) / (LU_CHMAX > 0 ? LU_CHMAX : 1);
+    static constexpr int LU_CH = (1 + D::NH + LU_NCH - 1) / LU_NCH;
+    static constexpr size_t smem_bytes =
+        WS ? sizeof(double) * (lu_off + D::NU * D::NU + (D::NU + 1) * LU_CH) : bytes;   // of it in shared memory
+    static_assert(!WS || LU_CHMAX >= 1, "the LU factors and one column fit shared memory");
 };
 
 // Resident elements per SM: the kernel is latency-bound (barrier-separated phases, a 40-step
@@ -846,13 +853,50 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
             bool tc_go = false;          // the unpivoted mixed solve passed its check: Schur product next
             __syncthreads();
             if constexpr (L::WS) {
-                // the system in memory: Gauss-Jordan with partial pivoting, then the solution rows
-                // (row s_piv[k] holds unknown k) into natural order
-                block_gauss_jordan<NT, true>(s_SD, NU, s_R, NU, NU, 1 + NH, s_piv, s_rowused, s_slot, s_bad);
-                double *s_perm = wk + L::d_perm;
-                for (int t = tid; t < NU * (1 + NH); t += NT) s_perm[t] = s_R[s_piv[t % NU] + NU * (t / NU)];
+                // LU with partial pivoting of SD in shared memory (dgesv's factorisation), then the
+                // 1 + NH right-hand sides in chunks: gathered in the pivot order, forward and back
+                // substitution in shared memory, the solution written straight to s_R
+                constexpr int NU1 = NU + 1, CH = L::LU_CH;
+                double *l_LU = reinterpret_cast<double *>(sm) + L::lu_off, *l_B = l_LU + NU * NU;
+                int *ip = s_rowvar;                      // row of SD that ends up at position i
+                for (int t = tid; t < NU * NU; t += NT) l_LU[t] = s_SD[t];
                 __syncthreads();
-                for (int t = tid; t < NU * (1 + NH); t += NT) s_R[t] = s_perm[t];
+                block_lu<NT>(l_LU, NU, NU, s_piv, s_bad);
+                if (tid == 0) {
+                    for (int i = 0; i < NU; i++) ip[i] = i;
+                    for (int k = 0; k < NU; k++) {
+                        const int q = s_piv[k], t = ip[k];
+                        ip[k] = ip[q];
+                        ip[q] = t;
+                    }
+                }
+                __syncthreads();
+                for (int c0 = 0; c0 < 1 + NH; c0 += CH) {
+                    const int nc = (1 + NH - c0) < CH ? (1 + NH - c0) : CH;
+                    for (int t = tid; t < NU * nc; t += NT) {
+                        const int i = t % NU, j = t / NU;
+                        l_B[i + NU1 * j] = s_R[ip[i] + NU * (c0 + j)];
+                    }
+                    __syncthreads();
+                    for (int k = 0; k < NU - 1; k++) {       // L y = P b (unit lower triangle)
+                        const int m = NU - k - 1;
+                        for (int t = tid; t < m * nc; t += NT) {
+                            const int i = k + 1 + t % m, j = t / m;
+                            l_B[i + NU1 * j] -= l_LU[i + NU * k] * l_B[k + NU1 * j];
+                        }
+                        __syncthreads();
+                    }
+                    for (int k = NU - 1; k >= 0; k--) {      // U x = y: row k is final at step k
+                        const double ukk = l_LU[k + NU * k];
+                        for (int t = tid; t < (k + 1) * nc; t += NT) {
+                            const int i = t % (k + 1), j = t / (k + 1);
+                            const double xk = l_B[k + NU1 * j] / ukk;
+                            if (i == k) s_R[k + NU * (c0 + j)] = xk;
+                            else l_B[i + NU1 * j] -= l_LU[i + NU * k] * xk;
+                        }
+                        __syncthreads();
+                    }
+                }
             } else if (force_piv) {
                 gj_regs<NU, 1 + NH, NT, 8, true>(s_SD, s_R, s_pcol, s_diag, s_rowvar, s_gslot, s_bad);
             } else {
@@ -1180,7 +1224,7 @@ static int launch_t(const Arg &p, int ne, cudaStream_t st, int grid_req) {
     const int dev = current_device(), nsm = sm_count_of(dev);
     int per_sm = per_sm_cache[dev < kMaxDevices ? dev : 0].load(std::memory_order_relaxed);
     if (per_sm < 1) {
-        // a plan in the global workspace wants the largest L1 (the smallest shared-memory carveout)
+        // a plan in the global workspace wants the largest L1 next to its shared memory
         if (L::WS && cudaFuncSetAttribute((const void *)kern, cudaFuncAttributePreferredSharedMemoryCarveout, 0) !=
                          cudaSuccess)
             return -10;

@@ -310,11 +310,15 @@ def main():
     ap.add_argument("--no-buckets", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"])
     ap.add_argument("--n", type=int, default=None, help="squares/cubes per side (smaller profiling cases)")
+    ap.add_argument("--porder", type=int, default=None, help="polynomial degree (another bucket of the workload)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.config])
     if args.n is not None:
         wl["kw"] = dict(wl["kw"], n=args.n)
         wl["desc"] = wl["desc"] + f" [reduced: n={args.n} per side]"
+    if args.porder is not None:
+        wl["kw"] = dict(wl["kw"], porder=args.porder)
+        wl["desc"] = wl["desc"].rsplit("p=", 1)[0] + f"p={args.porder}" + (f" [reduced: n={args.n} per side]" if args.n else "")
     if args.impl == "reference":
         return run_reference(args, wl)
 
@@ -405,7 +409,7 @@ def main():
         achieved_tf = cnt["flops"] * ne / avg_kern_s / 1e12
         achieved_gbs = cnt["bytes"] * ne / avg_kern_s / 1e9
         traffic = profile_traffic(f"elemental_kernel_{wl['name']}", "mixed" if use_mixed else "fp64")
-        if traffic is not None and args.n is not None:
+        if traffic is not None and (args.n is not None or args.porder is not None):
             traffic = None                           # the summary is for the full-size workload
         roof = {"bound": "tensor", "pipe": "fp64", "achieved": achieved_tf, "peak": fp64_peak,
                 "unit": "TFLOP/s", "frac": achieved_tf / fp64_peak,

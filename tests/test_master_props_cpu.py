@@ -24,7 +24,7 @@ import pytest
 from hdg_b200.master import gaussquad, mkmaster, mkshape
 
 G = Path(__file__).resolve().parent / "golden"
-COMPILED = [(2, 1), (2, 2), (2, 3), (2, 4), (3, 1), (3, 2)]
+COMPILED = [(2, 1), (2, 2), (2, 3), (2, 4), (3, 1), (3, 2), (3, 3)]
 
 
 def _exact(exps):

@@ -311,7 +311,13 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"])
     ap.add_argument("--n", type=int, default=None, help="squares/cubes per side (smaller profiling cases)")
     ap.add_argument("--porder", type=int, default=None, help="polynomial degree (another bucket of the workload)")
+    ap.add_argument("--serve-c5", type=int, default=0, metavar="N",
+                    help="only the serving measurement on N requests of the full C5 distribution (n 24-180)")
     args = ap.parse_args()
+    if args.serve_c5 > 0:
+        import torch
+        print(json.dumps(serve_c5(torch, args.serve_c5)), flush=True)
+        return 0
     wl = dict(WORKLOADS[args.config])
     if args.n is not None:
         wl["kw"] = dict(wl["kw"], n=args.n)
@@ -622,6 +628,29 @@ def serve_mix(torch, count=16, slots=8, ordering="mdf"):
                           "elements": int(sum(r.problem.mesh.ne for r in c5_conc_reqs)),
                           "concurrent": c5_conc, "sequential": c5_seq, "concurrent_shared_launches": c5_comb,
                           "speedup_solves_per_s": c5_conc["solves_per_s"] / c5_seq["solves_per_s"]}}
+
+
+def serve_c5(torch, count, slots=16, ordering="mdf"):
+    """The C5 serving distribution over its full size range: count requests of 2D n x n x 2
+    triangles with n 24-180 (1,152-64,800 elements), p 1-4, Mach 0.3-0.8, half Euler / half NS
+    Re 200-2000, Poisson arrivals at 20/s, served with continuous admission on `slots` slots,
+    against the same requests back to back.  Newton to 1e-10, MDF BILU(0)-GMRES."""
+    from hdg_b200.serve import Server, request_mix
+    kw = dict(nmin=24, nmax=180, pmin=1, pmax=4, rate=20.0)
+    Server(slots=slots, ordering=ordering).serve(request_mix(40, 8, **dict(kw, nmax=60)), realtime=False)
+    from hdg_b200.serve import SolveRequest
+    seq_reqs = request_mix(41, count, **kw)
+    conc_reqs = [SolveRequest(r.rid, r.problem, arrival=r.arrival) for r in seq_reqs]   # the same inputs
+    seq = Server(slots=1, ordering=ordering).serve_sequential(seq_reqs)
+    conc = Server(slots=slots, ordering=ordering).serve(conc_reqs)
+    same = all(a.UDG is not None and b.UDG is not None and np.array_equal(a.UDG, b.UDG)
+               and np.array_equal(a.UH, b.UH) for a, b in zip(seq_reqs, conc_reqs))
+    return {"serve_c5": {"mix": f"C5: {count} requests, 2D n x n x 2 with n 24-180, p 1-4, M 0.3-0.8, half Euler / "
+                                "half NS Re 200-2000, Poisson 20/s (seed 41)",
+                         "elements": int(sum(r.problem.mesh.ne for r in conc_reqs)), "slots": slots,
+                         "ordering": ordering, "newton_tol": 1e-10,
+                         "concurrent": conc, "sequential": seq, "identical_alone_vs_mix": bool(same),
+                         "speedup_solves_per_s": conc["solves_per_s"] / seq["solves_per_s"]}}
 
 
 def shared_launch(torch, count=24, n=6, p=3, steps=20):

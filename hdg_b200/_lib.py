@@ -57,7 +57,8 @@ class HdgxSolveOpts(ct.Structure):
 class HdgxSolveReport(ct.Structure):
     _fields_ = [("iterations", ct.c_int), ("converged", ct.c_int), ("ncolors", ct.c_int),
                 ("residuals", ct.c_double * (HDGX_SOLVE_MAXIT + 1)), ("alphas", ct.c_double * HDGX_SOLVE_MAXIT),
-                ("gmres_iters", ct.c_int * HDGX_SOLVE_MAXIT), ("gmres_relres", ct.c_double * HDGX_SOLVE_MAXIT)]
+                ("gmres_iters", ct.c_int * HDGX_SOLVE_MAXIT), ("gmres_relres", ct.c_double * HDGX_SOLVE_MAXIT),
+                ("graph_assemblies", ct.c_int)]
 
 
 class HdgxAssemblyMap(ct.Structure):

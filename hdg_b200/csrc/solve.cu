@@ -215,7 +215,8 @@ struct DevPool {
     }
 };
 
-double norm2(size_t n, const double *x, double *part, double *out, cudaStream_t st) {
+// |x| into out[0] (two kernels, no synchronisation)
+void norm2_launch(size_t n, const double *x, double *part, double *out, cudaStream_t st) {
     const int nsm = sm_count_of(current_device());
     size_t g = (n + 255) / 256;
     if (g > (size_t)nsm * 8) g = (size_t)nsm * 8;
@@ -223,11 +224,25 @@ double norm2(size_t n, const double *x, double *part, double *out, cudaStream_t 
     if (g < 1) g = 1;
     dot_partial_kernel<<<(unsigned)g, 256, 0, st>>>(n, x, x, part);
     dot_final_kernel<<<1, 256, 0, st>>>((int)g, part, out, 1);
+}
+
+double read_scalar(const double *d, cudaStream_t st) {
     double h = 0.0;
-    cudaMemcpyAsync(&h, out, sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
     return h;
 }
+
+// The assembly chain of one Newton solve as a CUDA graph, launched for every assembly after the
+// first: the inputs and outputs sit at fixed device addresses for the whole solve.
+struct ChainGraph {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~ChainGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (g) cudaGraphDestroy(g);
+    }
+};
 
 }  // namespace
 
@@ -321,8 +336,8 @@ int solve_impl(const hdgx_master *m, const hdgx_app *app, const hdgx_mesh *mesh,
     const unsigned gU = (unsigned)std::min<size_t>((nU + 255) / 256, (size_t)nsm * 8);
     const unsigned gH = (unsigned)std::min<size_t>((nH + 255) / 256, (size_t)nsm * 8);
 
-    // hdg_assemble.m: returns |F| or a negative status
-    auto assemble = [&](double *res) -> int {
+    // hdg_assemble.m (trace gather, elemental kernel, block-CSR gather) and |F| into part[1024]
+    auto assemble_chain = [&]() -> int {
         int rc = hdgx_gather_uh(ncu, ndf, ne, mesh->elcon, UH, UHe, stream);
         if (rc) return rc;
         if (comb) {
@@ -338,7 +353,44 @@ int solve_impl(const hdgx_master *m, const hdgx_app *app, const hdgx_mesh *mesh,
         if (rc) return rc;
         rc = hdgx_globalassembly(&A, &map, ncu, npf, nfe, mesh->elcon, AE, FE, Hg, Rg, stream);
         if (rc) return rc;
-        *res = norm2(nH, Rg, part, part + 1024, st);
+        norm2_launch(nH, Rg, part, part + 1024, st);
+        return 0;
+    };
+    // After the first assembly (which also does every kernel's first-use set-up), the chain is
+    // captured once into a graph on the solve's stream (thread-local capture; only on a
+    // non-blocking stream, which the legacy default stream never waits on, and not with a
+    // combiner, whose batching synchronises on the host).  A capture that fails leaves the
+    // plain launches in use.
+    ChainGraph chain;
+    bool chain_tried = comb != nullptr;
+    int graph_runs = 0;
+    auto capture_chain = [&]() {
+        chain_tried = true;
+        unsigned flags = 0;
+        if (!st || cudaStreamGetFlags(st, &flags) != cudaSuccess || !(flags & cudaStreamNonBlocking)) return;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        const int rc = assemble_chain();
+        const cudaError_t e = cudaStreamEndCapture(st, &chain.g);
+        if (rc || e != cudaSuccess || !chain.g || cudaGraphInstantiate(&chain.exec, chain.g, 0) != cudaSuccess) {
+            if (chain.g) cudaGraphDestroy(chain.g);
+            chain.g = nullptr;
+            chain.exec = nullptr;
+            cudaGetLastError();
+        }
+    };
+    // returns |F| or a negative status
+    auto assemble = [&](double *res) -> int {
+        if (chain.exec) {
+            if (cudaGraphLaunch(chain.exec, st) != cudaSuccess) return -12;
+            graph_runs++;
+        } else if (int rc = assemble_chain()) {
+            return rc;
+        }
+        *res = read_scalar(part + 1024, st);
+        if (!chain_tried) capture_chain();
         return 0;
     };
 
@@ -408,6 +460,7 @@ int solve_impl(const hdgx_master *m, const hdgx_app *app, const hdgx_mesh *mesh,
     r.iterations = it;
     r.converged = rel <= opts->tol;
     r.ncolors = A.ncolors;
+    r.graph_assemblies = graph_runs;
     if (rep) *rep = r;
     return cudaGetLastError() == cudaSuccess ? 0 : -12;
 }

@@ -406,5 +406,6 @@ def hdgx_solve(master, mesh, app, UDG, UH, SH=None, tol=1e-10, maxiter=16, gmres
     n = rep.iterations
     report = dict(iterations=n, converged=bool(rep.converged), levels=rep.ncolors,
                   residuals=list(rep.residuals[:n + 1]), alphas=list(rep.alphas[:n]),
-                  gmres_iters=list(rep.gmres_iters[:n]), gmres_relres=list(rep.gmres_relres[:n]))
+                  gmres_iters=list(rep.gmres_iters[:n]), gmres_relres=list(rep.gmres_relres[:n]),
+                  graph_assemblies=rep.graph_assemblies)
     return dU.numpy(), dH.numpy(), report

@@ -381,6 +381,7 @@ typedef struct {
     double alphas[HDGX_SOLVE_MAXIT];          /* line-search step lengths */
     int gmres_iters[HDGX_SOLVE_MAXIT];
     double gmres_relres[HDGX_SOLVE_MAXIT];
+    int graph_assemblies;     /* assemblies replayed from the CUDA graph of the assembly chain */
 } hdgx_solve_report;
 
 /* Newton solve of kernel/hdg_solve.m:84-176 on the device: assembly (hdg_assemble.m), BILU(0)-
@@ -390,7 +391,9 @@ typedef struct {
  * whose q part is taken as zero (hdg_solve.m:62-63, no wave formulation).  app->getdqdg must be
  * 1 (returns -2 otherwise; the Python composition also runs getdqdg = 0).  Workspace comes from a private stream-ordered memory pool of the library (one per device) and
  * is released into it before returning; the pool keeps up to 8 GiB of freed memory for later
- * calls.  The call synchronises the stream (it reads residual norms on the host). */
+ * calls.  The call synchronises the stream (it reads residual norms on the host).  On a
+ * non-blocking stream the assembly chain (trace gather, elemental kernel, block-CSR gather, |F|)
+ * is captured into a CUDA graph after the first assembly and replayed for the others. */
 int hdgx_solve(const hdgx_master *master, const hdgx_app *app, const hdgx_mesh *mesh, double *UDG, double *UH,
                const double *SH, const hdgx_solve_opts *opts, hdgx_solve_report *report, hdgx_stream_t stream);
 

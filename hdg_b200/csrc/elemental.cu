@@ -214,16 +214,24 @@ struct Plan {
     static constexpr bool TC = !WS && TC_PL != 0 && tc_a * 8 + 16 * TC_KC * 128 <= (int)(sizeof(double) * n_doubles) &&
                                TC_NP <= 256 && D::NU <= 64;
     static constexpr size_t bytes = sizeof(double) * n_doubles + sizeof(int) * n_ints;   // the whole plan
-    // WS: the local system is LU-factored in shared memory (the factors of SD, NU x NU, after the
-    // integers) and its right-hand sides solved in LU_NCH chunks of LU_CH columns (leading
-    // dimension NU + 1 against bank conflicts)
-    static constexpr int lu_off = al16((n_ints * (int)sizeof(int) + 7) / 8);         // doubles
+    // WS shared memory, in doubles after the integers: the face tables t_ft / t_fg (ws_tabs), SD
+    // (built there and LU-factored in place, at lu_off) followed by the right-hand sides solved in
+    // LU_NCH chunks of LU_CH columns (leading dimension NU + 1 against bank conflicts); before the
+    // SD build the same space holds the first scratch group [x_start, x_dead_end) (ws_dead: on
+    // top of SD when SD is built over that group, else after it)
+    static constexpr int ws_tabs = al16((n_ints * (int)sizeof(int) + 7) / 8);
+    static constexpr int lu_off = al16(ws_tabs + 2 * D::NGF * D::NPF);
+    static constexpr int ws_dead = SD_ALIAS ? lu_off : lu_off + D::NU * D::NU;
     static constexpr int LU_CHMAX = (227 * 1024 / 8 - lu_off - D::NU * D::NU) / (D::NU + 1);
     static constexpr int LU_NCH = (1 + D::NH + LU_CHMAX - 1) / (LU_CHMAX > 0 ? LU_CHMAX : 1);
     static constexpr int LU_CH = (1 + D::NH + LU_NCH - 1) / LU_NCH;
-    static constexpr size_t smem_bytes =
-        WS ? sizeof(double) * (lu_off + D::NU * D::NU + (D::NU + 1) * LU_CH) : bytes;   // of it in shared memory
+    static constexpr int ws_smem_doubles = (lu_off + D::NU * D::NU + (D::NU + 1) * LU_CH) >
+                                                   (ws_dead + x_dead_end - x_start)
+                                               ? lu_off + D::NU * D::NU + (D::NU + 1) * LU_CH
+                                               : ws_dead + x_dead_end - x_start;
+    static constexpr size_t smem_bytes = WS ? sizeof(double) * ws_smem_doubles : bytes;   // of it in shared memory
     static_assert(!WS || LU_CHMAX >= 1, "the LU factors and one column fit shared memory");
+    static_assert(!WS || smem_bytes <= 227 * 1024, "the shared-memory part of the plan fits");
 };
 
 // Resident elements per SM: the kernel is latency-bound (barrier-separated phases, a 40-step
@@ -272,7 +280,10 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     const int tid = threadIdx.x;
 
     const double *t_vt = L::TABLES ? wk + L::t_vt : P.shapvt, *t_vg = L::TABLES ? wk + L::t_vg : P.shapvg;
-    double *t_ft = wk + L::t_ft, *t_fg = wk + L::t_fg;
+    // WS: the face tables, SD and the first scratch group in shared memory (see Plan)
+    double *smd = reinterpret_cast<double *>(sm);
+    double *t_ft = L::WS ? smd + L::ws_tabs : wk + L::t_ft, *t_fg = L::WS ? t_ft + NGF * NPF : wk + L::t_fg;
+    double *xd = L::WS ? smd + L::ws_dead - L::x_start : wk;     // base of the first scratch group
     const double *__restrict__ t_mv = P.shapmv;   // geometry tables: read once per element from L1
     const double *__restrict__ t_mf = P.shapmf;
     int *perm = si + L::i_perm, *invp = si + L::i_invp;
@@ -317,16 +328,16 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
     }
 
     double *s_dg = wk + L::p_dg, *s_udg = wk + L::p_udg, *s_uh = wk + L::p_uh;
-    double *s_SD = wk + L::p_SD, *s_R = wk + L::p_R;
+    double *s_SD = L::WS ? smd + L::lu_off : wk + L::p_SD, *s_R = wk + L::p_R;
     double *s_MiC = wk + L::p_MiC, *s_MiE = wk + L::p_MiE, *s_MiRq = wk + L::p_MiRq;
-    double *s_Gp = wk + L::p_Gp, *s_Hp = wk + L::p_Hp, *s_Rh = wk + L::p_Rh, *s_M = wk + L::p_M;
+    double *s_Gp = wk + L::p_Gp, *s_Hp = wk + L::p_Hp, *s_Rh = wk + L::p_Rh, *s_M = xd + L::p_M;
     double *s_dudg = wk + L::p_dudg, *s_jv = wk + L::p_jv;
-    double *x_Xx = wk + L::x_Xx, *x_jac = wk + L::x_jac, *x_nl = wk + L::x_nl, *x_jf = wk + L::x_jf;
-    double *x_ug = wk + L::x_ug, *x_fu = wk + L::x_fu, *x_fuh = wk + L::x_fuh;
-    double *x_wrk = wk + L::x_wrk, *x_wrl = wk + L::x_wrl, *x_FH = wk + L::x_FH, *x_BH = wk + L::x_BH;
-    double *x_FHu = wk + L::x_FHu, *x_FHh = wk + L::x_FHh;
-    double *x_Zc = wk + L::x_Zc, *x_Ze = wk + L::x_Ze, *x_Zr = wk + L::x_Zr;
-    double *x_ZFc = wk + L::x_ZFc, *x_ZFe = wk + L::x_ZFe, *x_ZFr = wk + L::x_ZFr;
+    double *x_Xx = xd + L::x_Xx, *x_jac = xd + L::x_jac, *x_nl = xd + L::x_nl, *x_jf = xd + L::x_jf;
+    double *x_ug = xd + L::x_ug, *x_fu = xd + L::x_fu, *x_fuh = xd + L::x_fuh;
+    double *x_wrk = xd + L::x_wrk, *x_wrl = wk + L::x_wrl, *x_FH = xd + L::x_FH, *x_BH = xd + L::x_BH;
+    double *x_FHu = wk + L::x_FHu, *x_FHh = xd + L::x_FHh;
+    double *x_Zc = wk + L::x_Zc, *x_Ze = xd + L::x_Ze, *x_Zr = xd + L::x_Zr;
+    double *x_ZFc = wk + L::x_ZFc, *x_ZFe = xd + L::x_ZFe, *x_ZFr = xd + L::x_ZFr;
     int *s_piv = si + L::i_piv, *s_pivM = si + L::i_pivM, *s_bf = si + L::i_bf, *s_bad = si + L::i_bad;
     int *s_rowused = si + L::i_rowused, *s_rowvar = si + L::i_rowvar, *s_gslot = si + L::i_gslot;
     unsigned long long *s_slot = reinterpret_cast<unsigned long long *>(wk + L::d_slots);
@@ -857,10 +868,8 @@ __global__ void __launch_bounds__(NT, (min_blocks<D, VISC, MIXED>())) elemental_
                 // 1 + NH right-hand sides in chunks: gathered in the pivot order, forward and back
                 // substitution in shared memory, the solution written straight to s_R
                 constexpr int NU1 = NU + 1, CH = L::LU_CH;
-                double *l_LU = reinterpret_cast<double *>(sm) + L::lu_off, *l_B = l_LU + NU * NU;
+                double *l_LU = s_SD, *l_B = l_LU + NU * NU;   // SD is built in shared memory: factored in place
                 int *ip = s_rowvar;                      // row of SD that ends up at position i
-                for (int t = tid; t < NU * NU; t += NT) l_LU[t] = s_SD[t];
-                __syncthreads();
                 block_lu<NT>(l_LU, NU, NU, s_piv, s_bad);
                 if (tid == 0) {
                     for (int i = 0; i < NU; i++) ip[i] = i;

@@ -90,6 +90,10 @@ def lib():
 def _declare(L):
     i, d, v, p = ct.c_int, ct.c_double, ct.c_void_p, ct.POINTER
     L.hdgx_version.restype = i
+    L.hdgx_set_host_wait.restype = i
+    L.hdgx_set_host_wait.argtypes = [i]
+    L.hdgx_get_host_wait.restype = i
+    L.hdgx_get_host_wait.argtypes = []
     L.hdgx_status_str.restype = ct.c_char_p
     L.hdgx_status_str.argtypes = [i]
     L.hdgx_status_count.restype = i

@@ -1,7 +1,10 @@
 // capi.cu -- extern "C" entry points of libhdgx.so (declared in include/hdgx.h).
 #include <cuda_runtime.h>
 #include <math.h>
+#include <atomic>
 #include <mutex>
+#include <utility>
+#include <vector>
 #include "hdgx_common.cuh"
 
 namespace hdgx {
@@ -22,6 +25,36 @@ int schur_launch(int qform, int nd, int npv, int ncu, int nc, int ndf, int ne, c
                  const double *H, const double *Rq, const double *Ru, const double *Rh, double *DUDG,
                  double *DUDG_DUH, double *AE, double *FE, int *status, cudaStream_t st);
 
+std::atomic<int> g_host_wait{0};
+
+// Blocking-synchronisation events, per device, created on demand and reused
+static std::mutex g_wait_mu;
+static std::vector<std::pair<int, cudaEvent_t>> g_wait_free;
+
+cudaEvent_t host_wait_acquire() {
+    if (g_host_wait.load(std::memory_order_relaxed) != 1) return nullptr;
+    const int dev = current_device();
+    {
+        std::lock_guard<std::mutex> lk(g_wait_mu);
+        for (size_t i = 0; i < g_wait_free.size(); i++)
+            if (g_wait_free[i].first == dev) {
+                cudaEvent_t e = g_wait_free[i].second;
+                g_wait_free[i] = g_wait_free.back();
+                g_wait_free.pop_back();
+                return e;
+            }
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventBlockingSync | cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    return e;
+}
+
+void host_wait_release(cudaEvent_t ev) {
+    if (!ev) return;
+    std::lock_guard<std::mutex> lk(g_wait_mu);
+    g_wait_free.emplace_back(current_device(), ev);
+}
+
 __global__ void count_nonzero_kernel(const int *s, int n, int *out) {
     int c = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) c += (s[i] != 0);
@@ -33,6 +66,14 @@ __global__ void count_nonzero_kernel(const int *s, int n, int *out) {
 extern "C" {
 
 int hdgx_version(void) { return 10000; }
+
+int hdgx_set_host_wait(int mode) {
+    if (mode != 0 && mode != 1) return -1;
+    hdgx::g_host_wait.store(mode);
+    return 0;
+}
+
+int hdgx_get_host_wait(void) { return hdgx::g_host_wait.load(); }
 
 const char *hdgx_status_str(int code) {
     switch (code) {

@@ -292,6 +292,7 @@ int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const
     double h_scal[2] = {0.0, 0.0};
     double *h_nrmb = h_scal, *h_res = h_scal + 1;
     int rc = 0;
+    const HostWaiter wait;                        // sleeps until the GPU is done in blocking mode
     // a failed launch or copy ends the solve at the next synchronisation: no further work is queued
     auto synced = [&]() {
         const cudaError_t e = cudaStreamSynchronize(st);
@@ -301,6 +302,7 @@ int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const
     // pb = P^{-1} b, nrmb = |pb|
     if (int r = prec(b, t, pb)) rc = r;
     dot(N, pb, pb, gs.scal + 2, part, 1, st);
+    wait(st);
     cudaMemcpyAsync(h_nrmb, gs.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, st);
     synced();
     const double nrmb = *h_nrmb;
@@ -331,6 +333,7 @@ int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const
                 scale_div_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, hc + j + 1, w, w);
             }
             givens_kernel<<<1, 1, 0, st>>>(gs, m, j);
+            wait(st);
             cudaMemcpyAsync(h_res, gs.scal + 1, sizeof(double), cudaMemcpyDeviceToHost, st);
             if (!synced()) { fl = 3; stop = true; break; }
             res_rel = *h_res / nrmb;
@@ -347,6 +350,7 @@ int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const
         for (int i = 0; i < jdone; i++) axpy_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, gs.y + i, 1.0, V + N * i, x);
         if (stop) break;
     }
+    wait(st);
     synced();
     if (iters) *iters = iter;
     if (flag) *flag = fl;

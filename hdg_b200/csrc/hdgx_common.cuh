@@ -45,6 +45,25 @@ inline int sm_count_of(int dev) {
     }
     return n;
 }
+
+// How a host thread waits for the GPU where a solve reads a scalar back (GMRES residual, |F|):
+// mode 0 (default) as CUDA does by default, the thread spinning in the copy or synchronisation;
+// mode 1 (hdgx_set_host_wait) the thread first sleeps on a blocking-synchronisation event of a
+// pooled set until the GPU has reached that point, so that many concurrent solves do not keep as
+// many cores busy spinning.  Events come from a per-device pool (no create / destroy per solve).
+cudaEvent_t host_wait_acquire();         // nullptr in mode 0
+void host_wait_release(cudaEvent_t ev);
+struct HostWaiter {
+    cudaEvent_t ev;
+    HostWaiter() : ev(host_wait_acquire()) {}
+    ~HostWaiter() { host_wait_release(ev); }
+    HostWaiter(const HostWaiter &) = delete;
+    HostWaiter &operator=(const HostWaiter &) = delete;
+    // returns once the work queued on st so far has completed (mode 1), at once otherwise
+    void operator()(cudaStream_t st) const {
+        if (ev && cudaEventRecord(ev, st) == cudaSuccess) cudaEventSynchronize(ev);
+    }
+};
 }  // namespace hdgx
 
 namespace hdgx {

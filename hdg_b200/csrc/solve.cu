@@ -226,8 +226,9 @@ void norm2_launch(size_t n, const double *x, double *part, double *out, cudaStre
     dot_final_kernel<<<1, 256, 0, st>>>((int)g, part, out, 1);
 }
 
-double read_scalar(const double *d, cudaStream_t st) {
+double read_scalar(const double *d, cudaStream_t st, const HostWaiter &wait) {
     double h = 0.0;
+    wait(st);
     cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
     return h;
@@ -361,6 +362,7 @@ int solve_impl(const hdgx_master *m, const hdgx_app *app, const hdgx_mesh *mesh,
     // non-blocking stream, which the legacy default stream never waits on, and not with a
     // combiner, whose batching synchronises on the host).  A capture that fails leaves the
     // plain launches in use.
+    const HostWaiter wait;                        // how the host waits for the read-backs
     ChainGraph chain;
     bool chain_tried = comb != nullptr;
     int graph_runs = 0;
@@ -389,7 +391,7 @@ int solve_impl(const hdgx_master *m, const hdgx_app *app, const hdgx_mesh *mesh,
         } else if (int rc = assemble_chain()) {
             return rc;
         }
-        *res = read_scalar(part + 1024, st);
+        *res = read_scalar(part + 1024, st, wait);
         if (!chain_tried) capture_chain();
         return 0;
     };
@@ -410,6 +412,7 @@ int solve_impl(const hdgx_master *m, const hdgx_app *app, const hdgx_mesh *mesh,
             if (!C) return -13;
             if (int rc = hdgx_block_norms(&A, Hg, C, stream)) return rc;
             std::vector<double> Ch(nnzb);
+            wait(st);
             cudaMemcpyAsync(Ch.data(), C, sizeof(double) * nnzb, cudaMemcpyDeviceToHost, st);
             cudaStreamSynchronize(st);
             std::vector<int> o2u(nf), u2o(nf);
@@ -456,6 +459,7 @@ int solve_impl(const hdgx_master *m, const hdgx_app *app, const hdgx_mesh *mesh,
         r.residuals[it] = F;
         rel = F0 > 0.0 ? F / F0 : 0.0;
     }
+    wait(st);
     cudaStreamSynchronize(st);
     r.iterations = it;
     r.converged = rel <= opts->tol;

@@ -131,12 +131,15 @@ def latency_stats(reqs, t0):
 
 class Server:
     def __init__(self, slots=8, memory_budget=None, ordering="multicolor", mixed=False, restart=20, engine="native",
-                 max_bypass=4, combine=False, window_us=0):
+                 max_bypass=4, combine=False, window_us=0, blocking_waits=True):
         """max_bypass: how many later requests may be admitted ahead of a waiting request that
         does not fit yet (a large request waiting for memory does not block small ones behind
         it, but it is not overtaken more than this many times).  combine: the running requests'
         elemental evaluations of one degree and physics kind share launches (native engine,
-        FP64; ``solve.Combiner`` with ``window_us``)."""
+        FP64; ``solve.Combiner`` with ``window_us``).  blocking_waits: while ``serve`` runs, the
+        solves' host threads sleep on blocking-synchronisation events where they wait for the
+        GPU (``hdgx_set_host_wait(1)``) instead of each spinning on a core; ``serve_sequential``,
+        one solve at a time, keeps the spinning wait."""
         if combine and (engine != "native" or mixed):
             raise ValueError("shared launches need the native engine in FP64")
         if memory_budget is None:
@@ -146,6 +149,7 @@ class Server:
         self.ordering, self.mixed, self.restart, self.engine = ordering, mixed, restart, engine
         self.max_bypass = max_bypass
         self.combine, self.window_us = combine, window_us
+        self.blocking_waits = blocking_waits
         self.combiner_stats = None
 
     def serve(self, reqs, realtime=True):
@@ -160,6 +164,15 @@ class Server:
         if self.combine:
             from .solve import Combiner
             combiner = Combiner(self.window_us)
+        from ._lib import lib
+        prev_wait = lib().hdgx_get_host_wait()
+        lib().hdgx_set_host_wait(1 if self.blocking_waits else 0)
+        try:
+            return self._serve(reqs, realtime, pending, lock, state, streams, free_streams, dev, combiner)
+        finally:
+            lib().hdgx_set_host_wait(prev_wait)
+
+    def _serve(self, reqs, realtime, pending, lock, state, streams, free_streams, dev, combiner):
         t0 = time.perf_counter()
         threads = []
 

@@ -87,6 +87,15 @@ typedef struct {
 
 /* Library identity and error strings. */
 int hdgx_version(void);
+
+/* How host threads wait for the GPU where a solve reads a scalar back (each GMRES iteration's
+ * residual, |F| after each assembly, the MDF block norms): 0 (default) as CUDA does, the thread
+ * spinning until the copy completes; 1 the thread sleeps on a blocking-synchronisation event first
+ * (taken from a per-device pool the library keeps).  Mode 1 is for processes that run many solves
+ * at once, one host thread each (a serving loop): spinning threads then occupy as many cores and
+ * slow each other down.  Process-wide; no counterpart in the reference.  -1 for another mode. */
+int hdgx_set_host_wait(int mode);
+int hdgx_get_host_wait(void);
 const char *hdgx_status_str(int code);
 
 /* Number of nonzero entries of a device status[n] array (synchronises the stream). */

@@ -41,3 +41,14 @@ def test_version_and_status_strings():
     assert L.hdgx_version() >= 10000
     assert L.hdgx_status_str(0) == b"ok"
     assert b"unsupported" in L.hdgx_status_str(-3)
+
+
+def test_host_wait_mode_round_trip():
+    from hdg_b200 import _lib
+    L = _lib.lib()
+    prev = L.hdgx_get_host_wait()
+    assert prev in (0, 1)
+    assert L.hdgx_set_host_wait(2) == -1 and L.hdgx_set_host_wait(-1) == -1
+    assert L.hdgx_set_host_wait(1) == 0 and L.hdgx_get_host_wait() == 1
+    assert L.hdgx_set_host_wait(0) == 0 and L.hdgx_get_host_wait() == 0
+    L.hdgx_set_host_wait(prev)

@@ -62,3 +62,22 @@ def test_graph_captured_assembly_chain_is_bitwise_the_plain_one(name, kw, mixed)
     # every assembly after the first comes from the graph: at least one per Newton step
     assert r1["graph_assemblies"] == 0 and r2["graph_assemblies"] >= len(r2["residuals"]) - 1
     assert np.array_equal(U1, U2) and np.array_equal(H1, H2)
+
+
+def test_blocking_host_waits_change_nothing_but_the_wait():
+    """hdgx_set_host_wait(1): the host sleeps on blocking-synchronisation events before each
+    read-back; the solve's results are the same bits."""
+    from hdg_b200._lib import lib
+    from hdg_b200.solve import hdgx_solve
+    P = configs.c2(n=5, porder=2)
+    L = lib()
+    prev = L.hdgx_get_host_wait()
+    try:
+        L.hdgx_set_host_wait(0)
+        U0, H0, r0 = hdgx_solve(P.master, P.mesh, P.app, P.UDG, P.UH, P.SH, maxiter=6)
+        L.hdgx_set_host_wait(1)
+        U1, H1, r1 = hdgx_solve(P.master, P.mesh, P.app, P.UDG, P.UH, P.SH, maxiter=6)
+    finally:
+        L.hdgx_set_host_wait(prev)
+    assert r0["residuals"] == r1["residuals"] and r0["gmres_iters"] == r1["gmres_iters"]
+    assert np.array_equal(U0, U1) and np.array_equal(H0, H1)

@@ -616,6 +616,7 @@ def serve_mix(torch, count=16, slots=8, ordering="mdf"):
                                              for a, b in zip(c5_conc_reqs, c5_comb_reqs))
     torch.cuda.empty_cache()
     return {"requests": count, "slots": slots, "ordering": ordering, "newton_tol": 1e-10,
+            "host_waits": "concurrent runs: blocking-sync events (hdgx_set_host_wait(1)); back to back: CUDA's spinning wait",
             "mix": "2D n x n x 2, n 8-20, p 1-4, M 0.3-0.8, half Euler / half NS Re 200-2000, Poisson 20/s (seed 11)",
             "concurrent": s_conc, "sequential": s_seq, "identical_alone_vs_mix": bool(same),
             "speedup_solves_per_s": s_conc["solves_per_s"] / s_seq["solves_per_s"],

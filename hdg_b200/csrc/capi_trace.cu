@@ -259,12 +259,17 @@ size_t hdgx_gmres_workspace_bytes(const hdgx_bsr *A, int restart) {
     if (!A || restart < 1) return 0;
     const size_t N = (size_t)A->bs * A->nf;
     const size_t m = (size_t)restart;
-    return sizeof(double) * (N * (m + 1) + 3 * N + (m + 1) * m + 4 * (m + 1) + 8 + 2048 + 2) + 256;
+    return sizeof(double) * (N * (m + 1) + 3 * N + (m + 1) * m + 4 * (m + 1) + 8 + 2048 + 2 + m) + 256;
 }
 
 }  // extern "C"
 
 namespace hdgx {
+
+// GMRES steps launched between two host read-backs of the residual, for systems of at most
+// kGmresBatchMaxN unknowns (larger ones read back after every step)
+constexpr int kGmresBatch = 4;
+constexpr size_t kGmresBatchMaxN = 262144;
 
 int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const float *Mg32, const double *b,
                     double *x, int restart, double tol, int maxit, int *iters, int *flag, double *relres,
@@ -286,11 +291,12 @@ int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const
     double *part = gs.scal + 8;                   // [2048] partial sums
     unsigned *bar = reinterpret_cast<unsigned *>(part + 2048);   // grid barrier of the fused step
     int *bar_err = reinterpret_cast<int *>(bar + 1) + 1;         // [0] count, [1] generation, err
+    gs.hist = part + 2048 + 2;                    // [m] residual norm after each step of a cycle
     cudaMemsetAsync(bar, 0, 3 * sizeof(unsigned), st);
     // host scalars on the stack (pageable copies are stream-ordered and, unlike freeing
     // pinned memory, never synchronise the other streams of the device)
-    double h_scal[2] = {0.0, 0.0};
-    double *h_nrmb = h_scal, *h_res = h_scal + 1;
+    double h_scal[1 + kGmresBatch] = {};
+    double *h_nrmb = h_scal, *h_hist = h_scal + 1;
     int rc = 0;
     const HostWaiter wait;                        // sleeps until the GPU is done in blocking mode
     // a failed launch or copy ends the solve at the next synchronisation: no further work is queued
@@ -319,30 +325,42 @@ int gmres_bilu0_run(const hdgx_bsr *A, const double *Hg, const double *Mg, const
         gmres_init_kernel<<<1, 64, 0, st>>>(gs, m);
         int jdone = 0;
         bool stop = false;
-        for (int j = 0; j < m; j++) {
-            double *vj = V + N * j, *w = V + N * (j + 1);
-            if (int r = trace_matvec(A, Hg, vj, t, st)) rc = rc ? rc : r;
-            if (int r = prec(t, w2, w)) rc = rc ? rc : r;
-            double *hc = gs.H + (size_t)(m + 1) * j;
-            if (!mgs_fused(N, j + 1, V, w, hc, part, bar, bar_err, st)) {
-                for (int i = 0; i <= j; i++) {        // modified Gram-Schmidt (gmres_bilu0.m:59-63)
-                    dot(N, V + N * i, w, hc + i, part, 0, st);
-                    axpy_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, hc + i, -1.0, V + N * i, w);
+        // Steps between host read-backs: each step's residual norm is recorded on the device and
+        // read back `batch` steps at a time.  Steps past the one that stops write only what the
+        // update does not read (H columns, g entries and V columns beyond jdone), so the result is
+        // that of stopping there; one step at a time for large systems, whose steps are long.
+        const int batch = N <= kGmresBatchMaxN ? kGmresBatch : 1;
+        for (int j0 = 0; j0 < m && !stop;) {
+            int kb = m - j0 < batch ? m - j0 : batch;
+            if (kb > maxit - iter) kb = maxit - iter;
+            for (int j = j0; j < j0 + kb; j++) {
+                double *vj = V + N * j, *w = V + N * (j + 1);
+                if (int r = trace_matvec(A, Hg, vj, t, st)) rc = rc ? rc : r;
+                if (int r = prec(t, w2, w)) rc = rc ? rc : r;
+                double *hc = gs.H + (size_t)(m + 1) * j;
+                if (!mgs_fused(N, j + 1, V, w, hc, part, bar, bar_err, st)) {
+                    for (int i = 0; i <= j; i++) {        // modified Gram-Schmidt (gmres_bilu0.m:59-63)
+                        dot(N, V + N * i, w, hc + i, part, 0, st);
+                        axpy_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, hc + i, -1.0, V + N * i, w);
+                    }
+                    dot(N, w, w, hc + j + 1, part, 1, st);
+                    scale_div_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, hc + j + 1, w, w);
                 }
-                dot(N, w, w, hc + j + 1, part, 1, st);
-                scale_div_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, hc + j + 1, w, w);
+                givens_kernel<<<1, 1, 0, st>>>(gs, m, j);
             }
-            givens_kernel<<<1, 1, 0, st>>>(gs, m, j);
             wait(st);
-            cudaMemcpyAsync(h_res, gs.scal + 1, sizeof(double), cudaMemcpyDeviceToHost, st);
+            cudaMemcpyAsync(h_hist, gs.hist + j0, sizeof(double) * kb, cudaMemcpyDeviceToHost, st);
             if (!synced()) { fl = 3; stop = true; break; }
-            res_rel = *h_res / nrmb;
-            if (history && iter < maxit) history[iter] = res_rel;
-            iter++;
-            jdone = j + 1;
-            if (!isfinite(res_rel)) { fl = 3; stop = true; break; }
-            if (res_rel <= tol) { fl = 0; stop = true; break; }
-            if (iter >= maxit) { fl = 1; stop = true; break; }
+            for (int k = 0; k < kb && !stop; k++) {
+                res_rel = h_hist[k] / nrmb;
+                if (history && iter < maxit) history[iter] = res_rel;
+                iter++;
+                jdone = j0 + k + 1;
+                if (!isfinite(res_rel)) { fl = 3; stop = true; }
+                else if (res_rel <= tol) { fl = 0; stop = true; }
+                else if (iter >= maxit) { fl = 1; stop = true; }
+            }
+            j0 += kb;
         }
         if (rc) break;
         hess_solve_kernel<<<1, 1, 0, st>>>(gs, m, jdone);

@@ -246,6 +246,7 @@ int hdgx_gmres_dense(int nb, int nf, int nbf, const double *K, const int *f2f, c
     gs.g = gs.sn + (m + 1);
     gs.y = gs.g + (m + 1);
     gs.scal = gs.y + (m + 1);
+    gs.hist = nullptr;
     double *part = gs.scal + 8;                  // [1024 * (m + 1)] partial dot products
     const unsigned G = grid_n(N, 256) > 1024 ? 1024 : grid_n(N, 256);
     auto norm_into = [&](const double *v, double *out) {

@@ -9,11 +9,13 @@
 namespace hdgx {
 
 // Device state of restarted GMRES: Hessenberg H[(m+1), m] column-major, the Givens rotations
-// cs / sn [m+1], the rotated right-hand side g [m+1], the least-squares solution y [m+1], and
-// scal = [beta, |g_{j+1}|, scratch norm, ...].
+// cs / sn [m+1], the rotated right-hand side g [m+1], the least-squares solution y [m+1],
+// scal = [beta, |g_{j+1}|, scratch norm, ...], and (when not NULL) hist[m], the residual norm
+// |g_{j+1}| after each step j of the current cycle.
 struct GmresState {
     double *H, *cs, *sn, *g, *y;
     double *scal;
+    double *hist;
 };
 
 __global__ void givens_kernel(GmresState, int, int);

@@ -357,6 +357,7 @@ __global__ void givens_kernel(GmresState s, int m, int j) {
     s.g[j + 1] = -sn * s.g[j];
     s.g[j] = c * s.g[j];
     s.scal[1] = fabs(s.g[j + 1]);
+    if (s.hist) s.hist[j] = s.scal[1];
 }
 
 // Back substitution of the triangular Hessenberg system for y[0:k].  One thread.

@@ -125,6 +125,8 @@ def _declare(L):
     L.hdgx_block_norms.argtypes = [B, v, v, v]
     L.hdgx_mdf_ordering.restype = i
     L.hdgx_mdf_ordering.argtypes = [i, v, v, v, v, v]
+    L.hdgx_level_schedule.restype = i
+    L.hdgx_level_schedule.argtypes = [i, v, v, v, v, v, v]
     L.hdgx_matvec.restype = i
     L.hdgx_matvec.argtypes = [B, v, v, v, v]
     L.hdgx_bilu0_factor.restype = i

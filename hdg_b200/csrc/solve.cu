@@ -116,8 +116,11 @@ void build_multicolor(int nf, const long long *rowpts, const int *colind, HostPl
 // A sequential order o2u eliminated level by level: level(i) = 1 + max level of the
 // neighbours eliminated before i; rows of a level share no block, and ILU(0) factors depend
 // only on which of two coupled rows comes first, so the factors are the sequential order's.
-void build_levels(int nf, const long long *rowpts, const int *colind, const std::vector<int> &o2u,
-                  const std::vector<int> &u2o, HostPlan &hp) {
+// Level schedule of the sequential elimination order o2u: level(i) = 1 + the largest level of
+// the neighbours eliminated before i; rows grouped by level, by position inside a level.
+// level_ptr [nlev + 1] (room for nf + 1), rows [nf]; returns nlev.
+int level_schedule(int nf, const long long *rowpts, const int *colind, const int *o2u, const int *u2o,
+                   int *level_ptr, int *rows) {
     std::vector<int> lev(nf, 0);
     int nlev = 0;
     for (int j = 0; j < nf; j++) {
@@ -130,16 +133,24 @@ void build_levels(int nf, const long long *rowpts, const int *colind, const std:
         lev[i] = L + 1;
         nlev = std::max(nlev, L + 2);
     }
-    hp.ncolors = nlev;
-    hp.color_ptr.assign(nlev + 1, 0);
-    for (int i = 0; i < nf; i++) hp.color_ptr[lev[i] + 1]++;
-    for (int c = 0; c < nlev; c++) hp.color_ptr[c + 1] += hp.color_ptr[c];
-    std::vector<int> next(hp.color_ptr.begin(), hp.color_ptr.end() - 1);
-    hp.color_rows.resize(nf);
+    for (int c = 0; c <= nlev; c++) level_ptr[c] = 0;
+    for (int i = 0; i < nf; i++) level_ptr[lev[i] + 1]++;
+    for (int c = 0; c < nlev; c++) level_ptr[c + 1] += level_ptr[c];
+    std::vector<int> next(level_ptr, level_ptr + nlev);
     for (int j = 0; j < nf; j++) {                  // by level, then by position
         const int i = o2u[j];
-        hp.color_rows[next[lev[i]]++] = i;
+        rows[next[lev[i]]++] = i;
     }
+    return nlev;
+}
+
+void build_levels(int nf, const long long *rowpts, const int *colind, const std::vector<int> &o2u,
+                  const std::vector<int> &u2o, HostPlan &hp) {
+    std::vector<int> ptr(nf + 1);
+    hp.color_rows.resize(nf);
+    const int nlev = level_schedule(nf, rowpts, colind, o2u.data(), u2o.data(), ptr.data(), hp.color_rows.data());
+    hp.ncolors = nlev;
+    hp.color_ptr.assign(ptr.begin(), ptr.begin() + nlev + 1);
     hp.pos = u2o;
     // fixed-width dependency records of the one-launch sweeps (hdgx_bsr.sweep_plan)
     int dmax = 0;
@@ -482,4 +493,12 @@ extern "C" int hdgx_solve_combined(const hdgx_master *m, const hdgx_app *app, co
                                    hdgx_combiner *combiner, hdgx_stream_t stream) {
     if (!combiner) return -1;
     return solve_impl(m, app, mesh, UDG, UH, SH, opts, rep, combiner, stream);
+}
+
+extern "C" int hdgx_level_schedule(int nf, const long long *rowpts, const int *colind, const int *o2u, const int *u2o,
+                                   int *level_ptr, int *rows) {
+    if (nf < 0 || !rowpts || !colind || !o2u || !u2o || !level_ptr || !rows) return -1;
+    for (int j = 0; j < nf; j++)
+        if (o2u[j] < 0 || o2u[j] >= nf || u2o[o2u[j]] != j) return -1;   // not a permutation pair
+    return hdgx::level_schedule(nf, rowpts, colind, o2u, u2o, level_ptr, rows);
 }

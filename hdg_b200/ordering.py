@@ -104,23 +104,21 @@ def levels_of_order(rowpts, colind, o2u, u2o):
     neighbours eliminated before i.  ILU(0) factors depend only on which of two coupled
     rows comes first, so eliminating level by level (rows of a level share no block) gives
     exactly the factors of the sequential order.  Returns an Ordering whose "colours" are
-    the levels and whose positions are the sequential order's."""
+    the levels and whose positions are the sequential order's.  Computed by the library's
+    hdgx_level_schedule (host code; one pass over the order)."""
+    from ._lib import check, lib
     nf = len(o2u)
-    lev = np.zeros(nf, dtype=np.int64)
-    rp = np.asarray(rowpts)
-    ci = np.asarray(colind) - 1
-    u2o = np.asarray(u2o)
-    for j in range(nf):
-        i = int(o2u[j])
-        nb = ci[rp[i] + 1:rp[i + 1]]
-        low = nb[u2o[nb] < j]
-        lev[i] = lev[low].max() + 1 if low.size else 0
-    nlev = int(lev.max()) + 1
-    rows = np.lexsort((u2o, lev)).astype(np.int32)       # by level, then by position
-    counts = np.bincount(lev, minlength=nlev)
-    ptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
-    return Ordering(nlev, ptr, rows, np.asarray(u2o, dtype=np.int32), np.asarray(o2u, dtype=np.int32),
-                    np.asarray(u2o, dtype=np.int32))
+    rp = np.ascontiguousarray(rowpts, dtype=np.int64)
+    ci = np.ascontiguousarray(colind, dtype=np.int32)
+    o2u = np.ascontiguousarray(o2u, dtype=np.int32)
+    u2o = np.ascontiguousarray(u2o, dtype=np.int32)
+    ptr = np.zeros(nf + 1, dtype=np.int32)
+    rows = np.zeros(nf, dtype=np.int32)
+    nlev = lib().hdgx_level_schedule(nf, rp.ctypes.data, ci.ctypes.data, o2u.ctypes.data, u2o.ctypes.data,
+                                     ptr.ctypes.data, rows.ctypes.data)
+    if nlev < 0:
+        check(nlev, "hdgx_level_schedule")
+    return Ordering(nlev, ptr[:nlev + 1].copy(), rows, u2o.copy(), o2u.copy(), u2o.copy())
 
 
 def sweep_plan(order, rowpts, colind):

@@ -297,6 +297,15 @@ int hdgx_block_norms(const hdgx_bsr *A, const double *Hg, double *C, hdgx_stream
  * inverse (0-based, HOST).  Ties go to the lowest row, as MATLAB's min does. */
 int hdgx_mdf_ordering(int nf, const long long *rowpts, const int *colind, const double *C, int *o2u, int *u2o);
 
+/* Level schedule of the sequential elimination order o2u (u2o its inverse): level(i) = 1 + the
+ * largest level of the neighbours eliminated before i, so that eliminating level by level gives
+ * the factors of the sequential order (computeBILU0.m in the order of computeMDFordering.m).
+ * HOST arrays; rowpts [nf+1] 0-based, colind 1-based with the diagonal first; writes level_ptr
+ * [nlev + 1] (room for nf + 1) and rows [nf] (grouped by level, by position inside a level) and
+ * returns nlev, or -1 for bad arguments. */
+int hdgx_level_schedule(int nf, const long long *rowpts, const int *colind, const int *o2u, const int *u2o,
+                        int *level_ptr, int *rows);
+
 /* y = Hg x (kernel/matvec.m). */
 int hdgx_matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *y, hdgx_stream_t stream);
 

@@ -91,3 +91,41 @@ def test_sweep_plan_records_match_the_level_schedule():
             got = recs[q, c0:c0 + 2 * maxd].reshape(maxd, 2)
             assert [tuple(x) for x in got[:len(lst)]] == lst
             assert np.all(got[len(lst):] == -1)
+
+
+def test_level_schedule_is_the_sequential_orders_wavefront():
+    """hdgx_level_schedule: level(i) = 1 + the largest level of the neighbours eliminated
+    before i (restated here row by row), rows grouped by level and by position inside a level,
+    so that neighbours never share a level; bad permutations are refused."""
+    import ctypes as ct
+    from hdg_b200._lib import lib
+    from hdg_b200.ordering import levels_of_order
+    m = mkmesh_square(9, 9, 3, 0, 1.0, 1.0)
+    rp, ci = np.asarray(m.cbsr_rowpts), np.asarray(m.cbsr_colind)
+    rng = np.random.default_rng(11)
+    o2u = rng.permutation(m.nf).astype(np.int32)
+    u2o = np.empty_like(o2u)
+    u2o[o2u] = np.arange(m.nf, dtype=np.int32)
+    lev = np.zeros(m.nf, dtype=np.int64)
+    for j in range(m.nf):
+        i = o2u[j]
+        nb = ci[rp[i] + 1:rp[i + 1]] - 1
+        low = nb[u2o[nb] < j]
+        lev[i] = lev[low].max() + 1 if low.size else 0
+    lv = levels_of_order(rp, ci, o2u, u2o)
+    assert lv.ncolors == lev.max() + 1
+    want = np.lexsort((u2o, lev))
+    assert np.array_equal(lv.color_rows, want)
+    assert np.array_equal(np.diff(lv.color_ptr), np.bincount(lev))
+    for c in range(lv.ncolors):
+        rows = set(lv.color_rows[lv.color_ptr[c]:lv.color_ptr[c + 1]].tolist())
+        for i in rows:
+            assert not rows & set((ci[rp[i] + 1:rp[i + 1]] - 1).tolist())
+    bad = o2u.copy()
+    bad[0] = bad[1]
+    ptr = np.zeros(m.nf + 1, np.int32)
+    out = np.zeros(m.nf, np.int32)
+    rp64 = np.ascontiguousarray(rp, np.int64)
+    ci32 = np.ascontiguousarray(ci, np.int32)
+    assert lib().hdgx_level_schedule(m.nf, rp64.ctypes.data, ci32.ctypes.data, bad.ctypes.data, u2o.ctypes.data,
+                                     ptr.ctypes.data, out.ctypes.data) == -1

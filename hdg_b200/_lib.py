@@ -127,6 +127,8 @@ def _declare(L):
     L.hdgx_mdf_ordering.argtypes = [i, v, v, v, v, v]
     L.hdgx_level_schedule.restype = i
     L.hdgx_level_schedule.argtypes = [i, v, v, v, v, v, v]
+    L.hdgx_sweep_plan.restype = i
+    L.hdgx_sweep_plan.argtypes = [i, v, v, i, v, v, v, v, p(i)]
     L.hdgx_matvec.restype = i
     L.hdgx_matvec.argtypes = [B, v, v, v, v]
     L.hdgx_bilu0_factor.restype = i

@@ -144,6 +144,36 @@ int level_schedule(int nf, const long long *rowpts, const int *colind, const int
     return nlev;
 }
 
+// Record width of the one-launch sweeps: 4 or 6 (block, column) pairs per side, 0 when a row
+// has more than 6 off-diagonal blocks (no single-launch plan).
+int sweep_width(int nf, const long long *rowpts) {
+    int dmax = 0;
+    for (int i = 0; i < nf; i++) dmax = std::max<int>(dmax, (int)(rowpts[i + 1] - rowpts[i] - 1));
+    return dmax > 6 ? 0 : (dmax <= 4 ? 4 : 6);
+}
+
+// The single-launch sweep plan: [nlev + 1] level offsets, then per slot q of rows the record
+// (row i, its diagonal block rowpts[i], maxd (block, column) pairs of the neighbours eliminated
+// before i, maxd pairs of those eliminated after i), -1 padded, 0-based, neighbours in CSR order.
+void sweep_records(int nf, const long long *rowpts, const int *colind, int nlev, const int *level_ptr,
+                   const int *rows, const int *pos, int maxd, int *plan) {
+    const int RW = 2 + 4 * maxd;
+    for (int c = 0; c <= nlev; c++) plan[c] = level_ptr[c];
+    for (size_t t = 0; t < (size_t)nf * RW; t++) plan[nlev + 1 + t] = -1;
+    for (int q = 0; q < nf; q++) {
+        int *R = plan + (nlev + 1) + (size_t)q * RW;
+        const int i = rows[q];
+        R[0] = i;
+        R[1] = (int)rowpts[i];
+        int nb = 0, na = 0;
+        for (long long k = rowpts[i] + 1; k < rowpts[i + 1]; k++) {
+            const int j = colind[k] - 1;
+            if (pos[j] < pos[i]) { R[2 + 2 * nb] = (int)k; R[3 + 2 * nb] = j; nb++; }
+            else { R[2 + 2 * maxd + 2 * na] = (int)k; R[3 + 2 * maxd + 2 * na] = j; na++; }
+        }
+    }
+}
+
 void build_levels(int nf, const long long *rowpts, const int *colind, const std::vector<int> &o2u,
                   const std::vector<int> &u2o, HostPlan &hp) {
     std::vector<int> ptr(nf + 1);
@@ -153,25 +183,12 @@ void build_levels(int nf, const long long *rowpts, const int *colind, const std:
     hp.color_ptr.assign(ptr.begin(), ptr.begin() + nlev + 1);
     hp.pos = u2o;
     // fixed-width dependency records of the one-launch sweeps (hdgx_bsr.sweep_plan)
-    int dmax = 0;
-    for (int i = 0; i < nf; i++) dmax = std::max<int>(dmax, (int)(rowpts[i + 1] - rowpts[i] - 1));
-    if (dmax > 6) { hp.sweep.clear(); hp.sweep_maxd = 0; return; }
-    const int maxd = dmax <= 4 ? 4 : 6, RW = 2 + 4 * maxd;
+    const int maxd = sweep_width(nf, rowpts);
     hp.sweep_maxd = maxd;
-    hp.sweep.assign((size_t)(nlev + 1) + (size_t)nf * RW, -1);
-    for (int c = 0; c <= nlev; c++) hp.sweep[c] = hp.color_ptr[c];
-    for (int q = 0; q < nf; q++) {
-        int *R = hp.sweep.data() + (nlev + 1) + (size_t)q * RW;
-        const int i = hp.color_rows[q];
-        R[0] = i;
-        R[1] = (int)rowpts[i];
-        int nb = 0, na = 0;
-        for (long long k = rowpts[i] + 1; k < rowpts[i + 1]; k++) {
-            const int j = colind[k] - 1;
-            if (hp.pos[j] < hp.pos[i]) { R[2 + 2 * nb] = (int)k; R[3 + 2 * nb] = j; nb++; }
-            else { R[2 + 2 * maxd + 2 * na] = (int)k; R[3 + 2 * maxd + 2 * na] = j; na++; }
-        }
-    }
+    if (!maxd) { hp.sweep.clear(); return; }
+    hp.sweep.resize((size_t)(nlev + 1) + (size_t)nf * (2 + 4 * maxd));
+    sweep_records(nf, rowpts, colind, nlev, hp.color_ptr.data(), hp.color_rows.data(), hp.pos.data(), maxd,
+                  hp.sweep.data());
 }
 
 // A private stream-ordered memory pool per device.  Freed blocks stay in the pool up to
@@ -501,4 +518,13 @@ extern "C" int hdgx_level_schedule(int nf, const long long *rowpts, const int *c
     for (int j = 0; j < nf; j++)
         if (o2u[j] < 0 || o2u[j] >= nf || u2o[o2u[j]] != j) return -1;   // not a permutation pair
     return hdgx::level_schedule(nf, rowpts, colind, o2u, u2o, level_ptr, rows);
+}
+
+extern "C" int hdgx_sweep_plan(int nf, const long long *rowpts, const int *colind, int nlev, const int *level_ptr,
+                               const int *rows, const int *pos, int *plan, int *maxd) {
+    if (nf < 0 || nlev < 0 || !rowpts || !colind || !level_ptr || !rows || !pos || !maxd) return -1;
+    *maxd = hdgx::sweep_width(nf, rowpts);
+    if (*maxd == 0 || !plan) return 0;             // no plan, or the width asked for alone
+    hdgx::sweep_records(nf, rowpts, colind, nlev, level_ptr, rows, pos, *maxd, plan);
+    return 0;
 }

@@ -127,37 +127,20 @@ def sweep_plan(order, rowpts, colind):
     (row i, diagonal block rowpts[i], maxd (block, column) pairs of the neighbours eliminated
     before i, maxd pairs of those eliminated after i), -1 padded, 0-based, neighbours in CSR
     order.  Returns (plan int32 array, maxd), or (None, 0) when a row has more than 6
-    off-diagonal blocks."""
-    rp = np.asarray(rowpts, dtype=np.int64)
-    ci = np.asarray(colind, dtype=np.int64) - 1
+    off-diagonal blocks.  Built by the library's hdgx_sweep_plan (host code)."""
+    import ctypes as ct
+    from ._lib import check, lib
+    rp = np.ascontiguousarray(rowpts, dtype=np.int64)
+    ci = np.ascontiguousarray(colind, dtype=np.int32)
     nf = len(rp) - 1
-    deg = np.diff(rp) - 1
-    dmax = int(deg.max()) if nf else 0
-    if dmax > 6:
+    ptr = np.ascontiguousarray(order.color_ptr, dtype=np.int32)
+    rows = np.ascontiguousarray(order.color_rows, dtype=np.int32)
+    pos = np.ascontiguousarray(order.pos, dtype=np.int32)
+    maxd = ct.c_int(0)
+    args = (nf, rp.ctypes.data, ci.ctypes.data, int(order.ncolors), ptr.ctypes.data, rows.ctypes.data, pos.ctypes.data)
+    check(lib().hdgx_sweep_plan(*args, None, ct.byref(maxd)), "hdgx_sweep_plan")
+    if maxd.value == 0:
         return None, 0
-    maxd = 4 if dmax <= 4 else 6
-    pos = np.asarray(order.pos, dtype=np.int64)
-    rows = np.asarray(order.color_rows, dtype=np.int64)
-    row_of = np.repeat(np.arange(nf), np.diff(rp))
-    k = np.arange(len(ci))
-    off = k != rp[row_of]
-    k, i, j = k[off], row_of[off], ci[off]
-    later = (pos[j] > pos[i]).astype(np.int64)
-    # rank of each entry inside its (row, earlier/later) group, entries kept in CSR order
-    grp = i * 2 + later
-    srt = np.lexsort((k, grp))
-    g = grp[srt]
-    start = np.r_[0, np.flatnonzero(np.diff(g)) + 1]
-    first = np.repeat(start, np.diff(np.r_[start, len(g)]))
-    rank = np.arange(len(g)) - first
-    RW = 2 + 4 * maxd
-    recs = np.full((nf, RW), -1, dtype=np.int64)
-    slot = np.empty(nf, dtype=np.int64)
-    slot[rows] = np.arange(nf)
-    recs[:, 0] = rows
-    recs[:, 1] = rp[rows]
-    col = 2 + 2 * maxd * later[srt] + 2 * rank
-    recs[slot[i[srt]], col] = k[srt]
-    recs[slot[i[srt]], col + 1] = j[srt]
-    plan = np.concatenate([np.asarray(order.color_ptr, dtype=np.int64), recs.ravel()]).astype(np.int32)
-    return plan, maxd
+    plan = np.empty(int(order.ncolors) + 1 + nf * (2 + 4 * maxd.value), dtype=np.int32)
+    check(lib().hdgx_sweep_plan(*args, plan.ctypes.data, ct.byref(maxd)), "hdgx_sweep_plan")
+    return plan, maxd.value

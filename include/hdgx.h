@@ -306,6 +306,15 @@ int hdgx_mdf_ordering(int nf, const long long *rowpts, const int *colind, const 
 int hdgx_level_schedule(int nf, const long long *rowpts, const int *colind, const int *o2u, const int *u2o,
                         int *level_ptr, int *rows);
 
+/* The single-launch sweep plan of a level schedule (hdgx_bsr.sweep_plan), HOST arrays: *maxd = 4
+ * or 6 (0 when a row has more than 6 off-diagonal blocks: no plan, nothing written), and plan
+ * [nlev + 1 + nf * (2 + 4 maxd)] = the level offsets, then per slot q of rows the record (row i,
+ * its diagonal block rowpts[i], maxd (block, column) pairs of the neighbours with pos < pos[i],
+ * maxd pairs of those after it), -1 padded, 0-based, in CSR order.  Call with plan = NULL first
+ * to learn maxd.  0, or -1 for bad arguments. */
+int hdgx_sweep_plan(int nf, const long long *rowpts, const int *colind, int nlev, const int *level_ptr,
+                    const int *rows, const int *pos, int *plan, int *maxd);
+
 /* y = Hg x (kernel/matvec.m). */
 int hdgx_matvec(const hdgx_bsr *A, const double *Hg, const double *x, double *y, hdgx_stream_t stream);
 

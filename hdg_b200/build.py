@@ -14,11 +14,12 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-I", str(HERE.parent / "include")]
 
 
-# Per-file options.  elemental.cu: device functions that are not inlined (the boundary-flux
+# Per-file options.  elemental*.cu: device functions that are not inlined (the boundary-flux
 # routine, called from the rarely taken boundary branch of the face loop) are compiled for at
 # most 96 registers so that every elemental kernel instantiation (launch bounds of 96 to 255
 # registers per thread) can call them; the kernels' own limits come from their launch bounds.
-FILE_FLAGS = {"elemental.cu": ["-maxrregcount=96"]}
+def file_flags(name):
+    return ["-maxrregcount=96"] if name.startswith("elemental") else []
 
 
 def sources():
@@ -43,7 +44,7 @@ def build(verbose=False, force=False, jobs=None):
     for src in sources():
         obj = objdir / (src.stem + ".o")
         objs.append(obj)
-        cmd = [NVCC, *FLAGS, *FILE_FLAGS.get(src.name, []), "-dc", "-c", str(src), "-o", str(obj)]
+        cmd = [NVCC, *FLAGS, *file_flags(src.name), "-dc", "-c", str(src), "-o", str(obj)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))

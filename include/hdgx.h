@@ -424,16 +424,18 @@ typedef struct {
 int hdgx_solve(const hdgx_master *master, const hdgx_app *app, const hdgx_mesh *mesh, double *UDG, double *UH,
                const double *SH, const hdgx_solve_opts *opts, hdgx_solve_report *report, hdgx_stream_t stream);
 
-/* Shared elemental launches across concurrent solves (serving).  A combiner collects the assemblies
- * of the hdgx_solve_combined calls that run at the same time (each on its own host thread and
- * stream) and evaluates each group of equal master tables and one physics kind (viscous or not)
- * as one hdgx_elemental_shared launch on one of the combiner's streams; every solve's results are bitwise
- * those of hdgx_solve.  The first submission of a batch waits until every attached solve of its
- * group has submitted or window_us microseconds have passed (0: it takes what is queued at once).  One
+/* Shared elemental launches across concurrent solves (serving).  A combiner collects the
+ * assemblies of the hdgx_solve_combined calls that run at the same time (each on its own host
+ * thread and stream) and evaluates each group of equal master tables and one physics kind
+ * (viscous or not) as one hdgx_elemental_shared launch on one of the combiner's streams (a group
+ * of one as its own launch on its own stream); every solve's results are bitwise those of
+ * hdgx_solve.  The first submission of a batch waits until every attached solve of its group has
+ * submitted or window_us microseconds have passed (0: it takes what is queued at once).  One
  * combiner serves one device (the current device at creation; -2 for solves on another).
  * hdgx_solve_combined: arguments of hdgx_solve plus the combiner; FP64 only (opts->mixed = 1
- * returns -2); the call reads the master tables once to key its group.  Destroy only when no
- * solve is attached (-1 otherwise).  No counterpart in the reference (kernel/hdg_solve.m solves one
+ * returns -2); the call reads the master tables once to key its group; its assembly chain is not
+ * replayed from a graph (the batching synchronises on the host).  Destroy only when no solve is
+ * attached (-1 otherwise).  No counterpart in the reference (kernel/hdg_solve.m solves one
  * problem per call). */
 int hdgx_combiner_create(int window_us, hdgx_combiner **out);
 int hdgx_combiner_destroy(hdgx_combiner *combiner);

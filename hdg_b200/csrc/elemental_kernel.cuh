@@ -255,7 +255,9 @@ template <class D, bool VISC, bool MIXED>
 constexpr int min_blocks() { return blocks_for(PlanSel<D, VISC, MIXED>::bytes); }
 template <class D, bool VISC, bool MIXED>
 constexpr int cta_threads() {
-    return min_blocks<D, VISC, MIXED>() == 4 ? 128 : (min_blocks<D, VISC, MIXED>() == 3 ? 192 : 256);
+    return PlanSel<D, VISC, MIXED>::WS ? 512
+                                       : (min_blocks<D, VISC, MIXED>() == 4 ? 128
+                                                                            : (min_blocks<D, VISC, MIXED>() == 3 ? 192 : 256));
 }
 
 // MIXED: the local elimination of the Jacobian columns runs in FP32 (with the identity

@@ -516,6 +516,8 @@ def main():
             line["newton"] = newton_step(P, torch, args)
         if not args.no_buckets and ws == 1:
             line["buckets"] = buckets_mixed_degree(torch, use_mixed)
+            if args.config == "c2":
+                line["tetrahedra"] = tetrahedra_sample(torch)
         if not args.no_serve and ws == 1:
             line["serve"] = serve_mix(torch)
             line["serve"]["shared_launch"] = shared_launch(torch)
@@ -574,6 +576,40 @@ def buckets_mixed_degree(torch, mixed, n=181):
     del eb
     torch.cuda.empty_cache()
     return out
+
+
+def tetrahedra_sample(torch, steps=5):
+    """The tetrahedral shapes beside the C2 line: one FP64 elemental evaluation of 3D Euler p = 2
+    on 16^3 x 6 = 24,576 tets (C4's shape at an eighth of its size) and of 3D Euler and NS p = 3
+    on 8^3 x 6 = 3,072 tets; ms and elements/s (CUDA events, 3 warm-up evaluations)."""
+    from hdg_b200 import configs
+    from hdg_b200.app import make_app
+    from hdg_b200.elemental import DArray, DeviceMaster, alloc_elemental_outputs, hdg_elemental
+    res = {}
+    for tag, n, p, re in (("c4_shape_p2_euler", 16, 2, np.inf), ("p3_euler", 8, 3, np.inf), ("p3_ns_re100", 8, 3, 100.0)):
+        P = configs.c4(n=n, porder=p)
+        P.app = make_app(3, re=re, minf=0.4, tau=2.0)
+        dm = DeviceMaster(P.master)
+        dg = DArray.from_numpy(P.mesh.dgnodes)
+        bf = DArray.from_numpy(P.mesh.bf, dtype=torch.int32)
+        u, uh, sh = DArray.from_numpy(P.UDG), DArray.from_numpy(P.uh_elem()), DArray.from_numpy(P.SH)
+        out = alloc_elemental_outputs(P.master, P.app, P.mesh.ne)
+        run = lambda: hdg_elemental(P.master, P.app, dg, bf, u, uh, sh, out=out, dmaster=dm)
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            run()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res[tag] = {"elements": P.mesh.ne, "ms_per_step": ms, "value": P.mesh.ne / (ms * 1e-3), "unit": "elements/s",
+                    "status_max": int(out.status.numpy().max())}
+        del out
+    torch.cuda.empty_cache()
+    return res
 
 
 def serve_mix(torch, count=16, slots=8, ordering="mdf"):

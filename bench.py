@@ -517,7 +517,10 @@ def main():
         if not args.no_buckets and ws == 1:
             line["buckets"] = buckets_mixed_degree(torch, use_mixed)
             if args.config == "c2":
-                line["tetrahedra"] = tetrahedra_sample(torch)
+                try:
+                    line["tetrahedra"] = tetrahedra_sample(torch)
+                except Exception as exc:         # an auxiliary leg: report it, keep the line
+                    line["tetrahedra"] = {"error": repr(exc)}
         if not args.no_serve and ws == 1:
             line["serve"] = serve_mix(torch)
             line["serve"]["shared_launch"] = shared_launch(torch)
